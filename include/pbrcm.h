@@ -1,0 +1,249 @@
+/*
+ * pbrcm.h -- C ABI of the B200 Reverse Cuthill-McKee engine (libpbrcm.so).
+ *
+ * Drop-in boundary for the GPU_BATCH path of GPUPeople/ParallelBatchRCM.
+ * Plain pointers and sizes only; no CUDA or C++ types in the signatures
+ * (streams are passed as void*).  Every call returns a pbrcm_status; nothing
+ * throws or exits.
+ *
+ * Conventions shared by every entry point
+ *  - A matrix is a square CSR pattern: row_ptr[n+1] and col_idx[nnz], uint32,
+ *    as the reference's CSR<T> holds it (include/CSR.h:43-75 there).  Values
+ *    are never read.  Rows may hold the diagonal and duplicate entries; the
+ *    valence of a node is its row length (include/Graph.h:57-60).
+ *  - The result is a permutation perm[k] = original node at new position k.
+ *    With reverse = 0 it is the Cuthill-McKee order the reference returns
+ *    (its -r flag is parsed but never applied, src/main.cpp:250); with
+ *    reverse = 1 it is that order reversed (RCM).  The permutation is
+ *    bit-identical to the reference's serial stable CPU RCM
+ *    (src/rcm_cpu.cpp:57-104, rcm_seq<true>) from the same start node.
+ *  - The automatic start node is the reference's pseudo-peripheral node
+ *    (src/simple_peripheral.cpp:92-141, findPeripheral with 32 output
+ *    nodes), computed on the GPU.
+ *  - Bandwidth is the reference's computeBandwidth (src/main.cpp:143-184);
+ *    initial bandwidth its checkBandwidth (src/main.cpp:114-129).  Profile
+ *    (envelope) has no counterpart in the reference: sum over rows r of the
+ *    reordered matrix of r minus its smallest column, clamped at 0.
+ *  - The graph must be connected (the reference's loader connects it,
+ *    include/Graph.h:160-263; pbrcm_load_mtx does the same).  A disconnected
+ *    input returns PBRCM_ERR_DISCONNECTED instead of the reference's endless
+ *    spin.
+ */
+#ifndef PBRCM_H
+#define PBRCM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define PBRCM_API __attribute__((visibility("default")))
+#else
+#define PBRCM_API
+#endif
+
+#define PBRCM_AUTO_START 0xFFFFFFFFu
+
+typedef enum pbrcm_status {
+    PBRCM_OK = 0,
+    PBRCM_ERR_ARG = 1,          /* bad argument or size out of range */
+    PBRCM_ERR_DISCONNECTED = 2, /* BFS from the start did not reach every node */
+    PBRCM_ERR_TIMEOUT = 3,      /* a bounded device-side wait ran out */
+    PBRCM_ERR_OOM = 4,          /* device or host allocation failed */
+    PBRCM_ERR_CUDA = 5,         /* a CUDA runtime call failed */
+    PBRCM_ERR_IO = 6,           /* file could not be opened or read */
+    PBRCM_ERR_FORMAT = 7,       /* malformed MatrixMarket / .hicsr input */
+    PBRCM_ERR_CHECK = 8,        /* a device-side bounds check fired */
+    PBRCM_ERR_BUSY = 9,         /* admission refused: over the memory cap */
+    PBRCM_ERR_NOT_FOUND = 10    /* unknown ticket */
+} pbrcm_status;
+
+/* Options of one reorder (the reference's CLI flags, src/main.cpp:245-256). */
+typedef struct pbrcm_options {
+    uint32_t reverse;         /* -r: 1 = RCM (reversed CM order), 0 = CM order */
+    uint32_t start_node;      /* -s: explicit start, or PBRCM_AUTO_START */
+    uint32_t stable;          /* -b: accepted for compatibility; the result is
+                                 always the stable order (std::sort's tie order
+                                 in the reference's non-stable path is
+                                 implementation-defined, src/rcm_cpu.cpp:96) */
+    uint32_t want_bandwidth;  /* -w: compute bandwidth, initial bandwidth, profile */
+    uint32_t peripheral_nodes;/* nodes kept per BFS pass (0 = 32, the reference default) */
+    uint32_t wait_limit_ms;   /* bound of every device-side wait (0 = 2000 ms) */
+    uint32_t debug_flags;     /* test hooks, 0 in production (PBRCM_DEBUG_*) */
+    uint32_t reserved;
+} pbrcm_options;
+
+/* debug_flags: a grid barrier that waits for one CTA more than the launch has,
+ * so that the bounded wait runs out and PBRCM_ERR_TIMEOUT comes back. */
+#define PBRCM_DEBUG_PHANTOM_CTA 0x1u
+
+typedef struct pbrcm_result {
+    int32_t status;              /* pbrcm_status of this matrix */
+    uint32_t start_node;         /* start actually used */
+    uint32_t peripheral_passes;  /* BFS passes of the start search (0 if given) */
+    uint32_t eccentricity;       /* eccentricity of the start from the search */
+    uint32_t levels;             /* BFS levels of the final order */
+    uint32_t placed;             /* nodes placed (n when connected) */
+    int64_t bandwidth;           /* of the result (-1 if not asked) */
+    int64_t initial_bandwidth;   /* of the input as stored (-1 if not asked) */
+    uint64_t profile;            /* of the result (0 if not asked) */
+    float device_ms;             /* device time of the reorder launch(es) */
+    float total_ms;              /* host wall time of the call */
+} pbrcm_result;
+
+/* Default options: reverse=1, automatic start, stable=1, want_bandwidth=1. */
+PBRCM_API void pbrcm_default_options(pbrcm_options* opts);
+
+/* Library version string. */
+PBRCM_API const char* pbrcm_version(void);
+
+/* Human-readable name of a status code. */
+PBRCM_API const char* pbrcm_status_string(int32_t status);
+
+/* ---------------------------------------------------------------------- */
+/* Context: device, stream and a growing device workspace reused by calls.  */
+/* ---------------------------------------------------------------------- */
+typedef struct pbrcm_context pbrcm_context;
+
+/* Creates a context on `device` (the caller's current device if < 0). */
+PBRCM_API int32_t pbrcm_context_create(int32_t device, pbrcm_context** ctx);
+PBRCM_API void pbrcm_context_destroy(pbrcm_context* ctx);
+
+/*
+ * One reorder from HOST buffers.  Replaces GPU_BATCH::rcm<T>
+ * (include/rcm_gpu_batch.h:40-41, src/device/rcm_gpu_batch.cu:42-112): copies
+ * the CSR to the device, runs start search + CM + reverse + bandwidth in one
+ * persistent launch, copies perm back.  perm_out holds n entries.
+ * ctx may be NULL (a process-wide context on the current device is used).
+ */
+PBRCM_API int32_t pbrcm_reorder(pbrcm_context* ctx, const uint32_t* row_ptr, const uint32_t* col_idx,
+                      uint32_t n, uint64_t nnz, const pbrcm_options* opts, uint32_t* perm_out,
+                      pbrcm_result* result);
+
+/*
+ * One reorder on DEVICE-resident buffers, enqueued on `stream` (a
+ * cudaStream_t, NULL = the context's stream); d_perm_out receives n entries.
+ * Synchronises the stream before returning so that `result` is filled.
+ */
+PBRCM_API int32_t pbrcm_reorder_device(pbrcm_context* ctx, const uint32_t* d_row_ptr, const uint32_t* d_col_idx,
+                             uint32_t n, uint64_t nnz, const pbrcm_options* opts, uint32_t* d_perm_out,
+                             pbrcm_result* result, void* stream);
+
+/*
+ * Start-node search alone.  Replaces SimplePeripheral::findPeripheral
+ * (include/simple_peripheral.h:46) on the GPU.  Host buffers.
+ */
+PBRCM_API int32_t pbrcm_find_peripheral(pbrcm_context* ctx, const uint32_t* row_ptr, const uint32_t* col_idx,
+                              uint32_t n, uint64_t nnz, uint32_t* start_out, uint32_t* passes_out,
+                              uint32_t* ecc_out);
+
+/*
+ * Bandwidth / profile of a permutation.  Replaces computeBandwidth
+ * (src/main.cpp:143-184) on the GPU; also returns checkBandwidth
+ * (src/main.cpp:114-129) of the input and the profile.  Host buffers.
+ * Returns PBRCM_ERR_ARG if perm is not a bijection (checkPermutation,
+ * src/main.cpp:186-226).
+ */
+PBRCM_API int32_t pbrcm_bandwidth(pbrcm_context* ctx, const uint32_t* row_ptr, const uint32_t* col_idx,
+                        uint32_t n, uint64_t nnz, const uint32_t* perm, int64_t* bandwidth,
+                        int64_t* initial_bandwidth, uint64_t* profile);
+
+/* ---------------------------------------------------------------------- */
+/* Many matrices in one persistent launch.                                 */
+/* ---------------------------------------------------------------------- */
+typedef struct pbrcm_matrix {
+    const uint32_t* row_ptr;  /* n+1 entries */
+    const uint32_t* col_idx;  /* nnz entries */
+    uint32_t n;
+    uint32_t reserved;
+    uint64_t nnz;
+    uint32_t* perm_out;       /* n entries */
+} pbrcm_matrix;
+
+/*
+ * Reorders `count` independent matrices (HOST buffers) with one persistent
+ * launch: the CSRs are packed into one device arena, small matrices run one
+ * CTA each, matrices above the autotuned cutoff run on cooperative teams.
+ * results[i] receives matrix i's result.  The reference has no batched form;
+ * each permutation equals the single-matrix result.
+ */
+PBRCM_API int32_t pbrcm_reorder_batch(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t count,
+                            const pbrcm_options* opts, pbrcm_result* results);
+
+/* Same on device-resident CSRs and device perm buffers (pointers in `mats`
+ * are device pointers; `mats` itself is a host array). */
+PBRCM_API int32_t pbrcm_reorder_batch_device(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t count,
+                                   const pbrcm_options* opts, pbrcm_result* results, void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* Serving session: continuous batching of reorder requests.               */
+/* ---------------------------------------------------------------------- */
+typedef struct pbrcm_session pbrcm_session;
+
+typedef struct pbrcm_session_config {
+    uint64_t memory_cap_bytes; /* admission cap on device bytes in flight (0 = 120 GB) */
+    uint32_t max_inflight;     /* most requests on the device at once (0 = 4096) */
+    uint32_t streams;          /* concurrent device streams (0 = 8) */
+    uint32_t reserved[4];
+} pbrcm_session_config;
+
+PBRCM_API int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg, pbrcm_session** s);
+PBRCM_API void pbrcm_session_destroy(pbrcm_session* s);
+
+/*
+ * Submits one request (HOST buffers, copied before return).  Returns
+ * PBRCM_ERR_BUSY if the request alone exceeds the memory cap; otherwise the
+ * request is queued and admitted as soon as memory and slots allow.
+ */
+PBRCM_API int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const uint32_t* col_idx,
+                             uint32_t n, uint64_t nnz, const pbrcm_options* opts, uint64_t* ticket);
+
+/*
+ * Polls a ticket: returns PBRCM_OK with perm_out (n entries) and result
+ * filled once done (*done = 1), or *done = 0 if still running.  A finished
+ * ticket is released by the first poll that returns it.
+ */
+PBRCM_API int32_t pbrcm_session_poll(pbrcm_session* s, uint64_t ticket, uint32_t* perm_out, pbrcm_result* result,
+                           int32_t* done);
+
+/* Blocks until every submitted request has finished. */
+PBRCM_API int32_t pbrcm_session_drain(pbrcm_session* s);
+
+/* Latency / throughput counters since creation. */
+typedef struct pbrcm_session_stats {
+    uint64_t submitted, completed;
+    uint64_t bytes_in_flight, peak_bytes_in_flight;
+    double p50_ms, p99_ms, max_ms;     /* submit -> completion latency */
+    double busy_s;                     /* wall time from first submit to last completion */
+} pbrcm_session_stats;
+
+PBRCM_API int32_t pbrcm_session_stats_get(pbrcm_session* s, pbrcm_session_stats* st);
+
+/* ---------------------------------------------------------------------- */
+/* Input boundary: MatrixMarket loader with the reference's semantics.     */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * Loads a MatrixMarket `coordinate` file like Graph<T>::load
+ * (include/Graph.h:266-332: COO.cpp:89-199 parse, CSR.cpp:170-200 sort by
+ * (row, col), prepareRCM symmetrize + connect) without writing .hicsr cache
+ * files.  *row_ptr and *col_idx are malloc'd; free them with pbrcm_free.
+ */
+PBRCM_API int32_t pbrcm_load_mtx(const char* path, uint32_t* n, uint64_t* nnz, uint32_t** row_ptr,
+                       uint32_t** col_idx);
+
+/* prepareRCM (include/Graph.h:74-264) on a caller CSR; outputs malloc'd. */
+PBRCM_API int32_t pbrcm_prepare_csr(const uint32_t* row_ptr, const uint32_t* col_idx, uint32_t n, uint64_t nnz,
+                          int32_t check_symmetry, uint64_t* nnz_out, uint32_t** row_ptr_out,
+                          uint32_t** col_idx_out);
+
+PBRCM_API void pbrcm_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PBRCM_H */

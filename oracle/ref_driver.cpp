@@ -1,0 +1,202 @@
+// ref_driver.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// A small command-line driver that links the reference's own, unmodified CPU
+// sources (rcm_cpu.cpp, batchWorker.cpp, simple_peripheral.cpp, CSR.cpp,
+// COO.cpp and main.cpp with its main() renamed) so that the oracle and the
+// golden fixtures can be pinned on the reference itself, and so that the
+// reference's CPU path can be timed as the CPU baseline.  Built by
+// oracle/Makefile into oracle/_ref/ (never committed).
+//
+// Commands (all integers little-endian u32 files):
+//   ref_rcm load <file.mtx> <outprefix>
+//       Graph<float>::load (Graph.h:266-332; writes its .hicsr caches next to
+//       the input, so callers pass a copy in a scratch directory), dumps the
+//       loaded CSR to <outprefix>.rp / <outprefix>.ci, then runs `analyze`.
+//   ref_rcm csr <rp> <ci> <outprefix> [start]
+//       Same analysis on a raw CSR taken as is (no prepareRCM).
+//   ref_rcm time <rp> <ci> <threads> <steps>
+//       Times <steps> reorders: findPeripheral + RealCPU::rcm<true> with
+//       <threads> workers (1 = the serial rcm_seq path, else CPU_BATCH with
+//       batch size 512 as main.cpp:456-483 runs it).
+// `analyze` = findPeripheral (simple_peripheral.cpp:92) unless a start is
+// given, RealCPU::rcm<true>(.., 1, 1) (rcm_cpu.cpp:110), computeBandwidth /
+// checkBandwidth / maxValency / checkPermutation (main.cpp:94-226); it writes
+// the permutation to <outprefix>.perm and prints one line "JSON {...}".
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "Graph.h"
+#include "rcm_cpu.h"
+#include "simple_peripheral.h"
+
+// main.cpp (compiled with -Dmain=pbrcm_reference_cli_main)
+int computeBandwidth(const Graph<float>& graph, std::vector<uint32_t>& permutation);
+int checkBandwidth(const Graph<float>& graph);
+int maxValency(const Graph<float>& graph);
+int checkPermutation(const std::vector<uint32_t>& permutation);
+
+namespace {
+
+struct NullBuf : std::streambuf {
+    int overflow(int c) override { return c; }
+};
+
+std::vector<uint32_t> readU32(const char* path)
+{
+    std::ifstream f(path, std::ios::binary);
+    if (!f)
+        throw std::runtime_error(std::string("cannot open ") + path);
+    f.seekg(0, std::ios::end);
+    size_t bytes = static_cast<size_t>(f.tellg());
+    f.seekg(0);
+    std::vector<uint32_t> v(bytes / 4);
+    f.read(reinterpret_cast<char*>(v.data()), static_cast<std::streamsize>(v.size() * 4));
+    return v;
+}
+
+void writeU32(const std::string& path, const uint32_t* p, size_t n)
+{
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char*>(p), static_cast<std::streamsize>(n * 4));
+}
+
+void fillGraph(Graph<float>& g, const std::vector<uint32_t>& rp, const std::vector<uint32_t>& ci)
+{
+    size_t n = rp.size() - 1;
+    g.csr.alloc(n, n, ci.size());
+    std::memcpy(g.csr.row_offsets.get(), rp.data(), rp.size() * 4);
+    std::memcpy(g.csr.col_ids.get(), ci.data(), ci.size() * 4);
+    for (size_t i = 0; i < ci.size(); ++i)
+        g.csr.data[i] = 1.0f;
+    g.alloc(n);
+}
+
+// Runs findPeripheral with std::cout captured, returning (start, passes, ecc)
+// parsed from its "Peripheral<iters, start, end, lastdist>" line
+// (simple_peripheral.cpp:132-133).
+void peripheral(const Graph<float>& g, uint32_t& start, uint32_t& passes, uint32_t& ecc, double& ms)
+{
+    NullBuf nb;
+    std::ostream null_out(&nb);
+    std::stringstream cap;
+    auto* old = std::cout.rdbuf(cap.rdbuf());
+    auto t0 = std::chrono::high_resolution_clock::now();
+    start = SimplePeripheral::findPeripheral(g, null_out, false);
+    auto t1 = std::chrono::high_resolution_clock::now();
+    std::cout.rdbuf(old);
+    ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    std::string s = cap.str();
+    size_t p = s.find("Peripheral<");
+    passes = ecc = 0;
+    if (p != std::string::npos) {
+        unsigned a = 0, b = 0, c = 0, d = 0;
+        if (std::sscanf(s.c_str() + p, "Peripheral<%u, %u, %u, %u>", &a, &b, &c, &d) == 4) {
+            passes = a;
+            ecc = d;
+        }
+    }
+}
+
+// Runs RealCPU::rcm with std::cout captured; returns the printed mean (ms) of
+// its 25 internal repetitions (rcm_cpu.cpp:138-140).
+double rcmTimed(Graph<float>& g, std::vector<unsigned>& perm, uint32_t start, unsigned threads)
+{
+    NullBuf nb;
+    std::ostream null_out(&nb);
+    std::stringstream cap;
+    auto* old = std::cout.rdbuf(cap.rdbuf());
+    if (threads <= 1)
+        RealCPU::rcm<true>(g, null_out, perm, start, 1, 1);
+    else
+        RealCPU::rcm<true>(g, null_out, perm, start, threads, 512);
+    std::cout.rdbuf(old);
+    std::string s = cap.str();
+    size_t p = s.find("duration: ");
+    double ms = -1.0;
+    if (p != std::string::npos)
+        ms = std::atof(s.c_str() + p + 10);
+    return ms;
+}
+
+int analyze(Graph<float>& g, const std::string& outprefix, long forced_start)
+{
+    uint32_t start = 0, passes = 0, ecc = 0;
+    double pms = 0.0;
+    if (forced_start >= 0)
+        start = static_cast<uint32_t>(forced_start);
+    else
+        peripheral(g, start, passes, ecc, pms);
+    std::vector<unsigned> perm;
+    double rms = rcmTimed(g, perm, start, 1);
+    writeU32(outprefix + ".perm", perm.data(), perm.size());
+    std::vector<uint32_t> p32(perm.begin(), perm.end());
+    int bw = computeBandwidth(g, p32);
+    int bw0 = checkBandwidth(g);
+    int mv = maxValency(g);
+    int ok = checkPermutation(p32);
+    std::printf("JSON {\"n\": %zu, \"nnz\": %zu, \"start\": %u, \"peripheral_passes\": %u, "
+                "\"ecc\": %u, \"bandwidth\": %d, \"initial_bandwidth\": %d, \"max_valency\": %d, "
+                "\"check_permutation\": %d, \"placed\": %zu, \"peripheral_ms\": %.4f, \"rcm_ms\": %.4f}\n",
+                g.csr.rows, g.csr.nnz, start, passes, ecc, bw, bw0, mv, ok, perm.size(), pms, rms);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv)
+{
+    try {
+        if (argc >= 4 && std::strcmp(argv[1], "load") == 0) {
+            Graph<float> g;
+            {
+                std::stringstream cap;
+                auto* old = std::cout.rdbuf(cap.rdbuf());
+                int st = g.load(argv[2]);
+                std::cout.rdbuf(old);
+                if (st != 0) {
+                    std::printf("JSON {\"error\": \"load failed\", \"status\": %d}\n", st);
+                    return 2;
+                }
+            }
+            std::string out = argv[3];
+            writeU32(out + ".rp", g.csr.row_offsets.get(), g.csr.rows + 1);
+            writeU32(out + ".ci", g.csr.col_ids.get(), g.csr.nnz);
+            return analyze(g, out, argc >= 5 ? std::atol(argv[4]) : -1);
+        }
+        if (argc >= 5 && std::strcmp(argv[1], "csr") == 0) {
+            Graph<float> g;
+            fillGraph(g, readU32(argv[2]), readU32(argv[3]));
+            return analyze(g, argv[4], argc >= 6 ? std::atol(argv[5]) : -1);
+        }
+        if (argc >= 6 && std::strcmp(argv[1], "time") == 0) {
+            Graph<float> g;
+            fillGraph(g, readU32(argv[2]), readU32(argv[3]));
+            unsigned threads = static_cast<unsigned>(std::atoi(argv[4]));
+            int steps = std::atoi(argv[5]);
+            for (int s = 0; s < steps; ++s) {
+                uint32_t start, passes, ecc;
+                double pms;
+                peripheral(g, start, passes, ecc, pms);
+                std::vector<unsigned> perm;
+                double rms = rcmTimed(g, perm, start, threads);
+                std::printf("JSON {\"step\": %d, \"threads\": %u, \"start\": %u, \"peripheral_ms\": %.4f, "
+                            "\"rcm_ms\": %.4f, \"reorder_ms\": %.4f}\n",
+                            s, threads, start, pms, rms, pms + rms);
+                std::fflush(stdout);
+            }
+            return 0;
+        }
+    } catch (std::exception& e) {
+        std::printf("JSON {\"error\": \"%s\"}\n", e.what());
+        return 3;
+    }
+    std::fprintf(stderr, "usage: ref_rcm load <mtx> <outprefix> [start] | csr <rp> <ci> <outprefix> [start] | "
+                         "time <rp> <ci> <threads> <steps>\n");
+    return 1;
+}

@@ -1,0 +1,453 @@
+// api.cpp -- C ABI of libpbrcm (include/pbrcm.h): contexts, single-matrix and
+// batched reorders, start search and bandwidth.  Host C++ over the CUDA
+// runtime; all device work is in kernels.cu.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/pbrcm.h"
+#include "context.h"
+#include "kernels.h"
+#include "types.h"
+
+using namespace pbrcm;
+
+namespace pbrcm {
+
+const char* kVersion = "pbrcm-b200 0.1 (sm_100a)";
+
+// ---------------------------------------------------------------------------
+int32_t map_status(uint32_t s)
+{
+    switch (s) {
+    case kOk: return PBRCM_OK;
+    case kErrArg: return PBRCM_ERR_ARG;
+    case kErrDisconnected: return PBRCM_ERR_DISCONNECTED;
+    case kErrTimeout: return PBRCM_ERR_TIMEOUT;
+    case kErrCheck: return PBRCM_ERR_CHECK;
+    default: return PBRCM_ERR_CHECK;
+    }
+}
+
+Options make_options(const pbrcm_options* o, uint32_t mode)
+{
+    pbrcm_options d;
+    pbrcm_default_options(&d);
+    if (!o)
+        o = &d;
+    Options opt{};
+    opt.start = o->start_node;
+    opt.reverse = o->reverse ? 1u : 0u;
+    opt.want_bw = o->want_bandwidth ? 1u : 0u;
+    opt.outnodes = o->peripheral_nodes ? o->peripheral_nodes : 32u;
+    opt.wait_ns = (unsigned long long)(o->wait_limit_ms ? o->wait_limit_ms : 2000u) * 1000000ull;
+    opt.phantom = (o->debug_flags & PBRCM_DEBUG_PHANTOM_CTA) ? 1u : 0u;
+    opt.mode = mode;
+    return opt;
+}
+
+void fill_result(const DevResult& r, const Options& opt, pbrcm_result* out)
+{
+    if (!out)
+        return;
+    out->status = map_status(r.status);
+    out->start_node = r.start;
+    out->peripheral_passes = r.passes;
+    out->eccentricity = r.ecc;
+    out->levels = r.levels;
+    out->placed = r.placed;
+    if (opt.want_bw && r.status == kOk && opt.mode == kModeFull) {
+        out->bandwidth = (int64_t)r.bandwidth;
+        out->initial_bandwidth = (int64_t)r.initial_bw;
+        out->profile = opt.reverse ? r.profile_hi : r.profile_lo;
+    } else {
+        out->bandwidth = -1;
+        out->initial_bandwidth = -1;
+        out->profile = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+static int env_int(const char* name, int dflt)
+{
+    const char* v = std::getenv(name);
+    return v && *v ? std::atoi(v) : dflt;
+}
+
+int32_t Context::init(int dev)
+{
+    if (dev < 0) {
+        if (cudaGetDevice(&dev) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+    }
+    device = dev;
+    if (cudaSetDevice(dev) != cudaSuccess)
+        return PBRCM_ERR_CUDA;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess)
+        return PBRCM_ERR_CUDA;
+    sms = prop.multiProcessorCount;
+    if (!prop.cooperativeLaunch)
+        return PBRCM_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess)
+        return PBRCM_ERR_CUDA;
+    if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess)
+        return PBRCM_ERR_CUDA;
+    if (cudaMalloc(&d_res, sizeof(DevResult)) != cudaSuccess || cudaMalloc(&d_gs, sizeof(GridSync)) != cudaSuccess)
+        return PBRCM_ERR_OOM;
+    if (cudaMallocHost(&h_res, sizeof(DevResult)) != cudaSuccess)
+        return PBRCM_ERR_OOM;
+    // team shape: variant and CTA count (PBRCM_TEAM_VARIANT / PBRCM_TEAM_CTAS override)
+    team_variant = env_int("PBRCM_TEAM_VARIANT", 2);
+    if (team_variant < 0 || team_variant >= kNumVariants)
+        team_variant = 2;
+    int maxc = team_max_ctas(team_variant, sms);
+    if (maxc <= 0)
+        return PBRCM_ERR_CUDA;
+    team_ctas = env_int("PBRCM_TEAM_CTAS", 0);
+    if (team_ctas <= 0 || team_ctas > maxc)
+        team_ctas = std::min(maxc, sms);
+    batch_variant = env_int("PBRCM_BATCH_VARIANT", 1);
+    if (batch_variant < 0 || batch_variant >= kNumVariants)
+        batch_variant = 1;
+    if (cudaMalloc(&d_agg, sizeof(unsigned long long) * (size_t)std::max(maxc, 1)) != cudaSuccess)
+        return PBRCM_ERR_OOM;
+    return PBRCM_OK;
+}
+
+Context::~Context()
+{
+    if (device >= 0)
+        cudaSetDevice(device);
+    if (stream)
+        cudaStreamSynchronize(stream);
+    for (void* p : {(void*)d_rp, (void*)d_ci, (void*)d_claim, (void*)d_perm, (void*)d_rec, (void*)d_hub,
+                    (void*)d_res, (void*)d_gs, (void*)d_agg, (void*)d_jobs, (void*)d_counter, (void*)d_bres,
+                    (void*)d_arena, (void*)d_agg_session})
+        if (p)
+            cudaFree(p);
+    if (h_res)
+        cudaFreeHost(h_res);
+    if (ev0)
+        cudaEventDestroy(ev0);
+    if (ev1)
+        cudaEventDestroy(ev1);
+    if (stream)
+        cudaStreamDestroy(stream);
+}
+
+template <typename T>
+static bool grow(T*& p, size_t& cap, size_t need)
+{
+    if (need <= cap && p)
+        return true;
+    if (p)
+        cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max(need, (size_t)1);
+    if (cudaMalloc(&p, sizeof(T) * want) != cudaSuccess) {
+        p = nullptr;
+        return false;
+    }
+    cap = want;
+    return true;
+}
+
+bool Context::ensure_single(uint32_t n, uint64_t nnz, bool inputs)
+{
+    if (inputs && (!grow(d_rp, cap_rp, (size_t)n + 1) || !grow(d_ci, cap_ci, (size_t)nnz)))
+        return false;
+    return grow(d_claim, cap_claim, n) && grow(d_rec, cap_rec, n) && grow(d_perm, cap_perm, n);
+}
+
+bool Context::ensure_hub(uint64_t nnz) { return grow(d_hub, cap_hub, 4 * (size_t)std::max<uint64_t>(nnz, 1)); }
+
+// Runs start search (+ CM + bandwidth) on device buffers already in place.
+// Enqueues on `st`, synchronises, and retries once with hub scratch.
+int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint64_t nnz, uint32_t* perm,
+                            const Options& opt, cudaStream_t st, DevResult* out, float* dev_ms)
+{
+    bool with_hub = false;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        MatrixView M{};
+        M.rp = rp;
+        M.ci = ci;
+        M.n = n;
+        M.nnz = (uint32_t)nnz;
+        M.claim = d_claim;
+        M.rec = d_rec;
+        M.perm = perm;
+        M.hub = with_hub ? d_hub : nullptr;
+        M.res = d_res;
+        if (cudaMemsetAsync(d_res, 0, sizeof(DevResult), st) != cudaSuccess ||
+            cudaMemsetAsync(d_gs, 0, sizeof(GridSync), st) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+        if (launch_validate(rp, ci, n, (uint32_t)nnz, d_res, sms, st) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+        cudaEventRecord(ev0, st);
+        cudaError_t e = launch_team(team_variant, M, opt, d_gs, d_agg, team_ctas, st);
+        cudaEventRecord(ev1, st);
+        if (e != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+        if (cudaMemcpyAsync(h_res, d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+        if (cudaStreamSynchronize(st) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+        if (dev_ms)
+            cudaEventElapsedTime(dev_ms, ev0, ev1);
+        *out = *h_res;
+        if (out->status == kNeedHub && !with_hub) {
+            if (!ensure_hub(nnz))
+                return PBRCM_ERR_OOM;
+            with_hub = true;
+            continue;
+        }
+        break;
+    }
+    return PBRCM_OK;
+}
+
+static int32_t check_sizes(uint32_t n, uint64_t nnz)
+{
+    if (n == 0 || n == 0xFFFFFFFFu || nnz >= 0xFFFFFFFFull)
+        return PBRCM_ERR_ARG;
+    return PBRCM_OK;
+}
+
+}  // namespace pbrcm
+
+// ---------------------------------------------------------------------------
+// process-wide default context (per device)
+// ---------------------------------------------------------------------------
+static std::mutex g_default_mu;
+static std::vector<pbrcm_context*> g_default;
+
+static pbrcm_context* default_context(int32_t* rc)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        *rc = PBRCM_ERR_CUDA;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    if ((int)g_default.size() <= dev)
+        g_default.resize(dev + 1, nullptr);
+    if (!g_default[dev]) {
+        pbrcm_context* c = nullptr;
+        *rc = pbrcm_context_create(dev, &c);
+        if (*rc != PBRCM_OK)
+            return nullptr;
+        g_default[dev] = c;
+    }
+    *rc = PBRCM_OK;
+    return g_default[dev];
+}
+
+#define PBRCM_CTX(ctx)                               \
+    int32_t rc_ctx_ = PBRCM_OK;                      \
+    if (!ctx)                                        \
+        ctx = default_context(&rc_ctx_);             \
+    if (!ctx)                                        \
+        return rc_ctx_;                              \
+    std::lock_guard<std::mutex> lk_(ctx->ctx.mu);    \
+    cudaSetDevice(ctx->ctx.device);
+
+extern "C" {
+
+void pbrcm_default_options(pbrcm_options* o)
+{
+    if (!o)
+        return;
+    std::memset(o, 0, sizeof(*o));
+    o->reverse = 1;
+    o->start_node = PBRCM_AUTO_START;
+    o->stable = 1;
+    o->want_bandwidth = 1;
+    o->peripheral_nodes = 32;
+    o->wait_limit_ms = 2000;
+}
+
+const char* pbrcm_version(void) { return pbrcm::kVersion; }
+
+const char* pbrcm_status_string(int32_t s)
+{
+    switch (s) {
+    case PBRCM_OK: return "ok";
+    case PBRCM_ERR_ARG: return "invalid argument";
+    case PBRCM_ERR_DISCONNECTED: return "graph not connected";
+    case PBRCM_ERR_TIMEOUT: return "device wait timed out";
+    case PBRCM_ERR_OOM: return "out of memory";
+    case PBRCM_ERR_CUDA: return "CUDA error";
+    case PBRCM_ERR_IO: return "I/O error";
+    case PBRCM_ERR_FORMAT: return "format error";
+    case PBRCM_ERR_CHECK: return "device check failed";
+    case PBRCM_ERR_BUSY: return "over memory cap";
+    case PBRCM_ERR_NOT_FOUND: return "unknown ticket";
+    default: return "unknown status";
+    }
+}
+
+int32_t pbrcm_context_create(int32_t device, pbrcm_context** out)
+{
+    if (!out)
+        return PBRCM_ERR_ARG;
+    *out = nullptr;
+    auto* c = new (std::nothrow) pbrcm_context();
+    if (!c)
+        return PBRCM_ERR_OOM;
+    int32_t rc = c->ctx.init(device);
+    if (rc != PBRCM_OK) {
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return PBRCM_OK;
+}
+
+void pbrcm_context_destroy(pbrcm_context* c) { delete c; }
+
+int32_t pbrcm_reorder(pbrcm_context* ctx, const uint32_t* row_ptr, const uint32_t* col_idx, uint32_t n, uint64_t nnz,
+                      const pbrcm_options* opts, uint32_t* perm_out, pbrcm_result* result)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    if (!row_ptr || (!col_idx && nnz) || !perm_out)
+        return PBRCM_ERR_ARG;
+    if (int32_t rc = check_sizes(n, nnz))
+        return rc;
+    PBRCM_CTX(ctx);
+    Context& C = ctx->ctx;
+    if (!C.ensure_single(n, nnz, true))
+        return PBRCM_ERR_OOM;
+    Options opt = make_options(opts, kModeFull);
+    cudaStream_t st = C.stream;
+    if (cudaMemcpyAsync(C.d_rp, row_ptr, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        (nnz && cudaMemcpyAsync(C.d_ci, col_idx, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, st) != cudaSuccess))
+        return PBRCM_ERR_CUDA;
+    DevResult r{};
+    float dms = 0.f;
+    int32_t rc = C.run_single(C.d_rp, C.d_ci, n, nnz, C.d_perm, opt, st, &r, &dms);
+    if (rc != PBRCM_OK)
+        return rc;
+    if (r.status == kOk) {
+        if (cudaMemcpyAsync(perm_out, C.d_perm, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+    }
+    fill_result(r, opt, result);
+    if (result) {
+        result->device_ms = dms;
+        result->total_ms =
+            std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return map_status(r.status);
+}
+
+int32_t pbrcm_reorder_device(pbrcm_context* ctx, const uint32_t* d_row_ptr, const uint32_t* d_col_idx, uint32_t n,
+                             uint64_t nnz, const pbrcm_options* opts, uint32_t* d_perm_out, pbrcm_result* result,
+                             void* stream)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    if (!d_row_ptr || (!d_col_idx && nnz) || !d_perm_out)
+        return PBRCM_ERR_ARG;
+    if (int32_t rc = check_sizes(n, nnz))
+        return rc;
+    PBRCM_CTX(ctx);
+    Context& C = ctx->ctx;
+    if (!C.ensure_single(n, nnz, false))
+        return PBRCM_ERR_OOM;
+    Options opt = make_options(opts, kModeFull);
+    cudaStream_t st = stream ? (cudaStream_t)stream : C.stream;
+    DevResult r{};
+    float dms = 0.f;
+    int32_t rc = C.run_single(d_row_ptr, d_col_idx, n, nnz, d_perm_out, opt, st, &r, &dms);
+    if (rc != PBRCM_OK)
+        return rc;
+    fill_result(r, opt, result);
+    if (result) {
+        result->device_ms = dms;
+        result->total_ms =
+            std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return map_status(r.status);
+}
+
+int32_t pbrcm_find_peripheral(pbrcm_context* ctx, const uint32_t* row_ptr, const uint32_t* col_idx, uint32_t n,
+                              uint64_t nnz, uint32_t* start_out, uint32_t* passes_out, uint32_t* ecc_out)
+{
+    if (!row_ptr || (!col_idx && nnz) || !start_out)
+        return PBRCM_ERR_ARG;
+    if (int32_t rc = check_sizes(n, nnz))
+        return rc;
+    PBRCM_CTX(ctx);
+    Context& C = ctx->ctx;
+    if (!C.ensure_single(n, nnz, true))
+        return PBRCM_ERR_OOM;
+    pbrcm_options o;
+    pbrcm_default_options(&o);
+    Options opt = make_options(&o, kModeStartOnly);
+    cudaStream_t st = C.stream;
+    if (cudaMemcpyAsync(C.d_rp, row_ptr, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        (nnz && cudaMemcpyAsync(C.d_ci, col_idx, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, st) != cudaSuccess))
+        return PBRCM_ERR_CUDA;
+    DevResult r{};
+    int32_t rc = C.run_single(C.d_rp, C.d_ci, n, nnz, C.d_perm, opt, st, &r, nullptr);
+    if (rc != PBRCM_OK)
+        return rc;
+    *start_out = r.start;
+    if (passes_out)
+        *passes_out = r.passes;
+    if (ecc_out)
+        *ecc_out = r.ecc;
+    return map_status(r.status);
+}
+
+int32_t pbrcm_bandwidth(pbrcm_context* ctx, const uint32_t* row_ptr, const uint32_t* col_idx, uint32_t n,
+                        uint64_t nnz, const uint32_t* perm, int64_t* bandwidth, int64_t* initial_bandwidth,
+                        uint64_t* profile)
+{
+    if (!row_ptr || (!col_idx && nnz) || !perm)
+        return PBRCM_ERR_ARG;
+    if (int32_t rc = check_sizes(n, nnz))
+        return rc;
+    PBRCM_CTX(ctx);
+    Context& C = ctx->ctx;
+    if (!C.ensure_single(n, nnz, true))
+        return PBRCM_ERR_OOM;
+    cudaStream_t st = C.stream;
+    if (cudaMemcpyAsync(C.d_rp, row_ptr, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        (nnz && cudaMemcpyAsync(C.d_ci, col_idx, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, st) !=
+                    cudaSuccess) ||
+        cudaMemcpyAsync(C.d_perm, perm, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemsetAsync(C.d_res, 0, sizeof(DevResult), st) != cudaSuccess)
+        return PBRCM_ERR_CUDA;
+    if (launch_validate(C.d_rp, C.d_ci, n, (uint32_t)nnz, C.d_res, C.sms, st) != cudaSuccess ||
+        launch_bandwidth(C.d_rp, C.d_ci, n, C.d_perm, C.d_claim, C.d_res, C.sms, st) != cudaSuccess ||
+        cudaMemcpyAsync(C.h_res, C.d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return PBRCM_ERR_CUDA;
+    const DevResult& r = *C.h_res;
+    if (r.status != kOk)
+        return map_status(r.status);
+    if (bandwidth)
+        *bandwidth = (int64_t)r.bandwidth;
+    if (initial_bandwidth)
+        *initial_bandwidth = (int64_t)r.initial_bw;
+    if (profile)
+        *profile = r.profile_lo;
+    return PBRCM_OK;
+}
+
+}  // extern "C"

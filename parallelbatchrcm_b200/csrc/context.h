@@ -1,0 +1,73 @@
+// context.h -- per-device state behind a pbrcm_context.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+
+#include <cuda_runtime.h>
+
+#include "types.h"
+
+namespace pbrcm {
+
+struct Context {
+    std::mutex mu;
+    int device = -1;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int team_variant = 2;   // kernel shape of the one-matrix team
+    int team_ctas = 0;      // CTAs of the one-matrix team
+    int batch_variant = 1;  // kernel shape of the one-CTA-per-matrix batch
+
+    // single-matrix buffers (grow only)
+    uint32_t* d_rp = nullptr;
+    size_t cap_rp = 0;
+    uint32_t* d_ci = nullptr;
+    size_t cap_ci = 0;
+    uint32_t* d_claim = nullptr;
+    size_t cap_claim = 0;
+    uint32_t* d_perm = nullptr;
+    size_t cap_perm = 0;
+    PosRec* d_rec = nullptr;
+    size_t cap_rec = 0;
+    uint32_t* d_hub = nullptr;
+    size_t cap_hub = 0;
+    DevResult* d_res = nullptr;
+    DevResult* h_res = nullptr;
+    GridSync* d_gs = nullptr;
+    unsigned long long* d_agg = nullptr;
+
+    // batch buffers (grow only)
+    MatrixView* d_jobs = nullptr;
+    size_t cap_jobs = 0;
+    uint32_t* d_counter = nullptr;
+    size_t cap_counter = 0;
+    DevResult* d_bres = nullptr;
+    size_t cap_bres = 0;
+    unsigned char* d_arena = nullptr;
+    size_t cap_arena = 0;
+
+    // per-stream aggregate arrays of the serving session's team launches
+    unsigned long long* d_agg_session = nullptr;
+    size_t cap_agg_session = 0;
+    unsigned long long* d_agg_session_slot(int stream_index);
+
+    int32_t init(int dev);
+    ~Context();
+    bool ensure_single(uint32_t n, uint64_t nnz, bool inputs);
+    bool ensure_hub(uint64_t nnz);
+    int32_t run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint64_t nnz, uint32_t* perm,
+                       const Options& opt, cudaStream_t st, DevResult* out, float* dev_ms);
+};
+
+int32_t map_status(uint32_t s);
+Options make_options(const struct pbrcm_options* o, uint32_t mode);
+void fill_result(const DevResult& r, const Options& opt, struct pbrcm_result* out);
+
+}  // namespace pbrcm
+
+struct pbrcm_context {
+    pbrcm::Context ctx;
+};

@@ -1,0 +1,333 @@
+// kernels.cu -- sm_100a kernels of the engine and their host launchers.
+//
+//   k_validate        one pass over row_ptr / col_idx (coalesced): CSR sanity
+//                     and the largest valence (decides whether hub scratch is
+//                     needed); a bad CSR never reaches the engine.
+//   k_reorder_team    one matrix, all CTAs of a cooperative launch: start
+//                     search + CM pass + reverse + bandwidth in one launch.
+//   k_reorder_batch   many matrices, one CTA per matrix, matrices handed out
+//                     by an atomic counter (largest first).
+//   k_bandwidth_*     bandwidth / profile of a caller permutation.
+#include <algorithm>
+#include <cstdio>
+
+#include "engine.cuh"
+#include "kernels.h"
+
+namespace pbrcm {
+
+// ---------------------------------------------------------------------------
+__device__ void validate_one(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci, uint32_t n,
+                             uint32_t nnz, DevResult* res, uint64_t tid, uint64_t stride)
+{
+    __shared__ uint32_t s_max[32];
+    uint32_t mx = 0;
+    bool bad = false;
+    for (uint64_t i = tid; i < n; i += stride) {
+        const uint32_t a = rp[i], b = rp[i + 1];
+        if (b < a || b > nnz)
+            bad = true;
+        else
+            mx = max(mx, b - a);
+    }
+    if (tid == 0 && (rp[0] != 0 || rp[n] != nnz))
+        bad = true;
+    for (uint64_t k = tid; k < nnz; k += stride)
+        if (ci[k] >= n)
+            bad = true;
+    if (bad)
+        set_status(res, kErrArg, 200);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0)
+        s_max[w] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t m = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i)
+            m = max(m, s_max[i]);
+        atomicMax(&res->maxdeg, m);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_validate(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                                                  uint32_t n, uint32_t nnz, DevResult* res)
+{
+    validate_one(rp, ci, n, nnz, res, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                 (uint64_t)gridDim.x * blockDim.x);
+}
+
+// one CTA per matrix
+__global__ void __launch_bounds__(256) k_validate_batch(const MatrixView* jobs, uint32_t njobs)
+{
+    for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
+        const MatrixView M = jobs[j];
+        validate_one(M.rp, M.ci, M.n, M.nnz, M.res, threadIdx.x, blockDim.x);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Early exits shared by the reorder kernels.  Returns true if the matrix must
+// not be processed.  Every CTA reads the same values, so all agree.
+template <int EMAX>
+__device__ __forceinline__ bool skip_matrix(const MatrixView& M, bool first_thread)
+{
+    if (read_status(M.res) != 0)
+        return true;
+    if (M.res->maxdeg > (uint32_t)EMAX && M.hub == nullptr) {
+        if (first_thread)
+            set_status(M.res, kNeedHub, 0);
+        return true;
+    }
+    return false;
+}
+
+template <int B, int EMAX>
+__global__ void __launch_bounds__(B, 1) k_reorder_team(MatrixView M, Options opt, GridSync* gs,
+                                                        unsigned long long* agg)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto& s = *reinterpret_cast<Smem<B, EMAX>*>(smem_raw);
+    if (skip_matrix<EMAX>(M, blockIdx.x == 0 && threadIdx.x == 0))
+        return;
+    Team team;
+    team.gs = gridDim.x > 1 ? gs : nullptr;
+    team.size = gridDim.x;
+    team.rank = blockIdx.x;
+    team.expected = gridDim.x + opt.phantom;
+    team.gen = 0;
+    team.wait_ns = opt.wait_ns;
+    team.res = M.res;
+    reorder_matrix<B, EMAX>(s, M, team, agg, opt);
+}
+
+template <int B, int EMAX>
+__global__ void __launch_bounds__(B) k_reorder_batch(const MatrixView* jobs, uint32_t njobs, uint32_t* counter,
+                                                     Options opt)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto& s = *reinterpret_cast<Smem<B, EMAX>*>(smem_raw);
+    while (true) {
+        if (threadIdx.x == 0)
+            s.bcast[7] = atomicAdd(counter, 1u);
+        __syncthreads();
+        const uint32_t j = s.bcast[7];
+        __syncthreads();
+        if (j >= njobs)
+            break;
+        const MatrixView M = jobs[j];
+        if (skip_matrix<EMAX>(M, threadIdx.x == 0))
+            continue;
+        Team team;
+        team.gs = nullptr;
+        team.size = 1;
+        team.rank = 0;
+        team.expected = 1;
+        team.gen = 0;
+        team.wait_ns = opt.wait_ns;
+        team.res = M.res;
+        reorder_matrix<B, EMAX>(s, M, team, nullptr, opt);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Bandwidth of a caller permutation: inverse (with bijection check), then rows.
+__global__ void __launch_bounds__(256) k_bw_inverse(const uint32_t* __restrict__ perm, uint32_t n, uint32_t* inv,
+                                                    DevResult* res)
+{
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = perm[k];
+        if (v >= n || atomicCAS(inv + v, kUnvisited, (uint32_t)k) != kUnvisited)
+            set_status(res, kErrArg, 300);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_bw_rows(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                                                 uint32_t n, const uint32_t* __restrict__ inv, DevResult* res)
+{
+    __shared__ unsigned long long tmp[9];
+    unsigned long long bw = 0, bw0 = 0, plo = 0, phi = 0;
+    if (read_status(res) == 0) {
+        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+             i += (uint64_t)gridDim.x * blockDim.x) {
+            const uint32_t a = rp[i], e = rp[i + 1];
+            if (a == e)
+                continue;
+            const uint32_t me = inv[i];
+            uint32_t mnr = kUnvisited, mxr = 0;
+            for (uint32_t k = a; k < e; ++k) {
+                const uint32_t p = inv[ci[k]];
+                mnr = min(mnr, p);
+                mxr = max(mxr, p);
+            }
+            const unsigned long long b1 = me >= mnr ? (unsigned long long)(me - mnr) : 0ull;
+            const unsigned long long b2 = mxr >= me ? (unsigned long long)(mxr - me) : 0ull;
+            bw = max(bw, max(b1, b2));
+            plo += b1;
+            phi += b2;
+            const uint32_t c0 = ci[a], c1 = ci[e - 1];
+            const unsigned long long i0 = i >= c0 ? i - c0 : 0, i1 = c1 >= i ? c1 - i : 0;
+            bw0 = max(bw0, max(i0, i1));
+        }
+    }
+    bw = block_reduce_max<256, unsigned long long>(bw, tmp);
+    bw0 = block_reduce_max<256, unsigned long long>(bw0, tmp);
+    plo = block_reduce_sum<256, unsigned long long>(plo, tmp);
+    phi = block_reduce_sum<256, unsigned long long>(phi, tmp);
+    if (threadIdx.x == 0) {
+        atomicMax(&res->bandwidth, bw);
+        atomicMax(&res->initial_bw, bw0);
+        atomicAdd(&res->profile_lo, plo);
+        atomicAdd(&res->profile_hi, phi);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+
+template <int B, int EMAX>
+struct Variant {
+    static size_t smem() { return sizeof(Smem<B, EMAX>); }
+    static cudaError_t prepare()
+    {
+        static cudaError_t once = [] {
+            cudaError_t e = cudaFuncSetAttribute(k_reorder_team<B, EMAX>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+            if (e != cudaSuccess)
+                return e;
+            return cudaFuncSetAttribute(k_reorder_batch<B, EMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem());
+        }();
+        return once;
+    }
+    static int team_max_ctas(int sms)
+    {
+        if (prepare() != cudaSuccess)
+            return 0;
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_reorder_team<B, EMAX>, B, smem()) != cudaSuccess)
+            return 0;
+        return nb * sms;
+    }
+    static int batch_max_ctas(int sms)
+    {
+        if (prepare() != cudaSuccess)
+            return 0;
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_reorder_batch<B, EMAX>, B, smem()) !=
+            cudaSuccess)
+            return 0;
+        return nb * sms;
+    }
+    static cudaError_t team(const MatrixView& M, const Options& opt, GridSync* gs, unsigned long long* agg, int ctas,
+                            cudaStream_t st)
+    {
+        cudaError_t e = prepare();
+        if (e != cudaSuccess)
+            return e;
+        MatrixView m = M;
+        Options o = opt;
+        void* args[] = {&m, &o, &gs, &agg};
+        return cudaLaunchCooperativeKernel((const void*)k_reorder_team<B, EMAX>, dim3(ctas), dim3(B), args, smem(),
+                                           st);
+    }
+    static cudaError_t batch(const MatrixView* jobs, uint32_t njobs, uint32_t* counter, const Options& opt, int ctas,
+                             cudaStream_t st)
+    {
+        cudaError_t e = prepare();
+        if (e != cudaSuccess)
+            return e;
+        k_reorder_batch<B, EMAX><<<ctas, B, smem(), st>>>(jobs, njobs, counter, opt);
+        return cudaGetLastError();
+    }
+};
+
+}  // namespace
+
+const VariantInfo kVariants[kNumVariants] = {
+    {128, 512},
+    {256, 1024},
+    {512, 2048},
+};
+
+#define PBRCM_DISPATCH(v, CALL)                     \
+    switch (v) {                                    \
+    case 0: return Variant<128, 512>::CALL;         \
+    case 1: return Variant<256, 1024>::CALL;        \
+    case 2: return Variant<512, 2048>::CALL;        \
+    default: break;                                 \
+    }
+
+size_t variant_smem(int v)
+{
+    PBRCM_DISPATCH(v, smem());
+    return 0;
+}
+
+int team_max_ctas(int v, int sms)
+{
+    PBRCM_DISPATCH(v, team_max_ctas(sms));
+    return 0;
+}
+
+int batch_max_ctas(int v, int sms)
+{
+    PBRCM_DISPATCH(v, batch_max_ctas(sms));
+    return 0;
+}
+
+cudaError_t launch_team(int v, const MatrixView& M, const Options& opt, GridSync* gs, unsigned long long* agg,
+                        int ctas, cudaStream_t st)
+{
+    PBRCM_DISPATCH(v, team(M, opt, gs, agg, ctas, st));
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_batch(int v, const MatrixView* jobs, uint32_t njobs, uint32_t* counter, const Options& opt,
+                         int ctas, cudaStream_t st)
+{
+    PBRCM_DISPATCH(v, batch(jobs, njobs, counter, opt, ctas, st));
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_validate(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint32_t nnz, DevResult* res,
+                            int sms, cudaStream_t st)
+{
+    uint64_t work = (uint64_t)n + nnz;
+    int blocks = (int)std::min<uint64_t>((work + 255) / 256, (uint64_t)sms * 8);
+    if (blocks < 1)
+        blocks = 1;
+    k_validate<<<blocks, 256, 0, st>>>(rp, ci, n, nnz, res);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_validate_batch(const MatrixView* jobs, uint32_t njobs, int sms, cudaStream_t st)
+{
+    int blocks = (int)std::min<uint32_t>(njobs, (uint32_t)sms * 8);
+    if (blocks < 1)
+        blocks = 1;
+    k_validate_batch<<<blocks, 256, 0, st>>>(jobs, njobs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bandwidth(const uint32_t* rp, const uint32_t* ci, uint32_t n, const uint32_t* perm, uint32_t* inv,
+                             DevResult* res, int sms, cudaStream_t st)
+{
+    int blocks = (int)std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)sms * 8);
+    if (blocks < 1)
+        blocks = 1;
+    cudaError_t e = cudaMemsetAsync(inv, 0xFF, sizeof(uint32_t) * (size_t)n, st);
+    if (e != cudaSuccess)
+        return e;
+    k_bw_inverse<<<blocks, 256, 0, st>>>(perm, n, inv, res);
+    k_bw_rows<<<blocks, 256, 0, st>>>(rp, ci, n, inv, res);
+    return cudaGetLastError();
+}
+
+}  // namespace pbrcm

@@ -1,0 +1,35 @@
+// kernels.h -- host-callable launchers of the engine kernels (kernels.cu).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "types.h"
+
+namespace pbrcm {
+
+// Kernel shape variants: threads per CTA (B) and edges per chunk (EMAX).
+struct VariantInfo {
+    int block;
+    int emax;
+};
+constexpr int kNumVariants = 3;
+extern const VariantInfo kVariants[kNumVariants];
+
+size_t variant_smem(int v);
+int team_max_ctas(int v, int sms);   // co-resident CTAs of the team kernel
+int batch_max_ctas(int v, int sms);  // resident CTAs of the batch kernel
+
+cudaError_t launch_validate(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint32_t nnz, DevResult* res,
+                            int sms, cudaStream_t st);
+cudaError_t launch_validate_batch(const MatrixView* jobs, uint32_t njobs, int sms, cudaStream_t st);
+cudaError_t launch_team(int v, const MatrixView& M, const Options& opt, GridSync* gs, unsigned long long* agg,
+                        int ctas, cudaStream_t st);
+cudaError_t launch_batch(int v, const MatrixView* jobs, uint32_t njobs, uint32_t* counter, const Options& opt,
+                         int ctas, cudaStream_t st);
+cudaError_t launch_bandwidth(const uint32_t* rp, const uint32_t* ci, uint32_t n, const uint32_t* perm, uint32_t* inv,
+                             DevResult* res, int sms, cudaStream_t st);
+
+}  // namespace pbrcm

@@ -1,0 +1,501 @@
+// session.cpp -- serving session: continuous batching of reorder requests.
+//
+// submit() copies a request's CSR into pinned staging and queues it.  A
+// worker thread admits queued requests in arrival order whenever the device
+// bytes in flight stay under the cap and a slot is free, and launches each one
+// at once on the next of S streams: stream-ordered device allocation, H2D,
+// validation, the reorder kernel (one CTA for small matrices, a cooperative
+// team for large ones or ones with hub rows), D2H of the permutation and the
+// result, an event.  Requests that arrive while others run are launched
+// immediately, so their kernels overlap on the device.  The worker retires
+// finished requests by polling their events, frees their memory and records
+// submit->completion latency.  The reference has no serving mode; each result
+// equals the single-matrix result for the same input.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/pbrcm.h"
+#include "context.h"
+#include "kernels.h"
+#include "types.h"
+
+using namespace pbrcm;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// Pinned host memory, recycled by size class (powers of two).
+class PinnedPool {
+public:
+    ~PinnedPool()
+    {
+        for (auto& kv : free_)
+            cudaFreeHost(kv.second);
+    }
+    void* get(size_t bytes, size_t& cap)
+    {
+        size_t c = 4096;
+        while (c < bytes)
+            c <<= 1;
+        auto it = free_.find(c);
+        if (it != free_.end()) {
+            void* p = it->second;
+            free_.erase(it);
+            cap = c;
+            return p;
+        }
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, c, cudaHostAllocDefault) != cudaSuccess)
+            return nullptr;
+        cap = c;
+        return p;
+    }
+    void put(void* p, size_t cap)
+    {
+        if (p)
+            free_.emplace(cap, p);
+    }
+
+private:
+    std::multimap<size_t, void*> free_;
+};
+
+struct Request {
+    uint64_t ticket = 0;
+    uint32_t n = 0;
+    uint64_t nnz = 0;
+    uint32_t maxdeg = 0;
+    Options opt{};
+    size_t dev_bytes = 0;
+    // pinned staging: [rp | ci | view | perm_out | result]
+    unsigned char* host = nullptr;
+    size_t host_cap = 0;
+    size_t off_rp = 0, off_ci = 0, off_view = 0, off_perm = 0, off_res = 0;
+    // device block: [rp | ci | claim | rec | perm | res | gs | counter | hub?]
+    unsigned char* dev = nullptr;
+    size_t d_rp = 0, d_ci = 0, d_claim = 0, d_rec = 0, d_perm = 0, d_res = 0, d_gs = 0, d_cnt = 0, d_hub = 0;
+    bool team = false;
+    int stream = 0;
+    cudaEvent_t ev = nullptr;
+    int state = 0;  // 0 queued, 1 running, 2 done
+    int32_t rc = PBRCM_OK;
+    Clock::time_point t_submit, t_done;
+};
+
+}  // namespace
+
+struct pbrcm_session {
+    Context* C = nullptr;
+    uint64_t cap_bytes = 0;
+    uint32_t max_inflight = 0;
+    std::vector<cudaStream_t> streams;
+    uint32_t next_stream = 0;
+    int small_variant = 1;
+    uint32_t team_cutoff_n = 1u << 18;
+    int team_ctas = 0;
+
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request*> queued;
+    std::vector<Request*> running;
+    std::unordered_map<uint64_t, Request*> all;
+    uint64_t next_ticket = 1;
+    uint64_t bytes_in_flight = 0, peak_bytes = 0;
+    uint64_t submitted = 0, completed = 0;
+    std::vector<double> lat_ms;
+    Clock::time_point t_first{}, t_last{};
+    bool have_first = false;
+    PinnedPool pinned;
+    std::atomic<bool> stop{false};
+    std::thread worker;
+    cudaMemPool_t pool = nullptr;
+
+    void run();
+    bool launch(Request* r);
+    void retire(Request* r);
+};
+
+namespace {
+
+size_t device_bytes(uint32_t n, uint64_t nnz, bool hub, size_t* offs)
+{
+    size_t o = 0;
+    offs[0] = o;  // rp
+    o = align16(o + 4 * ((size_t)n + 1));
+    offs[1] = o;  // ci
+    o = align16(o + 4 * (size_t)nnz);
+    offs[2] = o;  // claim
+    o = align16(o + 4 * (size_t)n);
+    offs[3] = o;  // rec
+    o = align16(o + 16 * (size_t)n);
+    offs[4] = o;  // perm
+    o = align16(o + 4 * (size_t)n);
+    offs[5] = o;  // res
+    o = align16(o + sizeof(DevResult));
+    offs[6] = (o + 127) & ~(size_t)127;  // gs
+    o = offs[6] + sizeof(GridSync);
+    offs[7] = o;  // counter (+ job view)
+    o = align16(o + 16 + sizeof(MatrixView));
+    offs[8] = o;  // hub
+    if (hub)
+        o = align16(o + 16 * std::max<uint64_t>(nnz, 1));
+    return o;
+}
+
+}  // namespace
+
+bool pbrcm_session::launch(Request* r)
+{
+    cudaStream_t st = streams[r->stream];
+    Context& c = *C;
+    if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->dev), r->dev_bytes, pool, st) != cudaSuccess)
+        return false;
+    unsigned char* D = r->dev;
+    MatrixView M{};
+    M.rp = reinterpret_cast<const uint32_t*>(D + r->d_rp);
+    M.ci = reinterpret_cast<const uint32_t*>(D + r->d_ci);
+    M.n = r->n;
+    M.nnz = (uint32_t)r->nnz;
+    M.claim = reinterpret_cast<uint32_t*>(D + r->d_claim);
+    M.rec = reinterpret_cast<PosRec*>(D + r->d_rec);
+    M.perm = reinterpret_cast<uint32_t*>(D + r->d_perm);
+    M.hub = r->team && r->maxdeg > (uint32_t)kVariants[c.team_variant].emax
+                ? reinterpret_cast<uint32_t*>(D + r->d_hub)
+                : nullptr;
+    M.res = reinterpret_cast<DevResult*>(D + r->d_res);
+    std::memcpy(r->host + r->off_view, &M, sizeof(M));
+    MatrixView* d_view = reinterpret_cast<MatrixView*>(D + r->d_cnt + 16);
+    uint32_t* d_counter = reinterpret_cast<uint32_t*>(D + r->d_cnt);
+    bool ok = cudaMemcpyAsync(D + r->d_rp, r->host + r->off_rp, 4 * ((size_t)r->n + 1), cudaMemcpyHostToDevice,
+                              st) == cudaSuccess;
+    if (r->nnz)
+        ok = ok && cudaMemcpyAsync(D + r->d_ci, r->host + r->off_ci, 4 * (size_t)r->nnz, cudaMemcpyHostToDevice,
+                                   st) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(D + r->d_res, 0, sizeof(DevResult), st) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(D + r->d_gs, 0, sizeof(GridSync) + 0, st) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(d_counter, 0, 16, st) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(d_view, r->host + r->off_view, sizeof(MatrixView), cudaMemcpyHostToDevice, st) ==
+                   cudaSuccess;
+    ok = ok && launch_validate(M.rp, M.ci, M.n, M.nnz, M.res, c.sms, st) == cudaSuccess;
+    if (r->team)
+        ok = ok && launch_team(c.team_variant, M, r->opt, reinterpret_cast<GridSync*>(D + r->d_gs),
+                               reinterpret_cast<unsigned long long*>(c.d_agg_session_slot(r->stream)), team_ctas,
+                               st) == cudaSuccess;
+    else
+        ok = ok && launch_batch(small_variant, d_view, 1, d_counter, r->opt, 1, st) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(r->host + r->off_perm, M.perm, 4 * (size_t)r->n, cudaMemcpyDeviceToHost, st) ==
+                   cudaSuccess;
+    ok = ok && cudaMemcpyAsync(r->host + r->off_res, M.res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) ==
+                   cudaSuccess;
+    ok = ok && cudaFreeAsync(r->dev, st) == cudaSuccess;
+    ok = ok && cudaEventRecord(r->ev, st) == cudaSuccess;
+    return ok;
+}
+
+void pbrcm_session::retire(Request* r)
+{
+    DevResult res;
+    std::memcpy(&res, r->host + r->off_res, sizeof(res));
+    r->rc = map_status(res.status);
+    r->state = 2;
+    r->t_done = Clock::now();
+    bytes_in_flight -= r->dev_bytes;
+    ++completed;
+    lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+    t_last = r->t_done;
+}
+
+void pbrcm_session::run()
+{
+    cudaSetDevice(C->device);
+    std::unique_lock<std::mutex> lk(mu);
+    while (!stop.load()) {
+        bool progress = false;
+        for (size_t i = 0; i < running.size();) {
+            Request* r = running[i];
+            if (cudaEventQuery(r->ev) == cudaSuccess) {
+                retire(r);
+                running[i] = running.back();
+                running.pop_back();
+                progress = true;
+            } else {
+                ++i;
+            }
+        }
+        while (!queued.empty() && running.size() < max_inflight) {
+            Request* r = queued.front();
+            if (bytes_in_flight + r->dev_bytes > cap_bytes && !running.empty())
+                break;
+            queued.pop_front();
+            r->stream = (int)(next_stream++ % streams.size());
+            bytes_in_flight += r->dev_bytes;
+            peak_bytes = std::max(peak_bytes, bytes_in_flight);
+            r->state = 1;
+            if (!launch(r)) {
+                r->rc = PBRCM_ERR_CUDA;
+                r->state = 2;
+                r->t_done = Clock::now();
+                bytes_in_flight -= r->dev_bytes;
+                ++completed;
+            } else {
+                running.push_back(r);
+            }
+            progress = true;
+        }
+        if (progress)
+            cv_done.notify_all();
+        if (running.empty() && queued.empty())
+            cv_work.wait(lk, [&] { return stop.load() || !queued.empty(); });
+        else if (!progress) {
+            lk.unlock();
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+            lk.lock();
+        }
+    }
+}
+
+// The team kernel needs a per-stream aggregate array; it lives in the context.
+namespace pbrcm {
+unsigned long long* Context::d_agg_session_slot(int s)
+{
+    const int maxc = team_max_ctas(team_variant, sms);
+    const size_t need = (size_t)(s + 1) * (size_t)std::max(maxc, 1);
+    if (need > cap_agg_session) {
+        // grown only from the worker before any launch on stream s is in flight
+        unsigned long long* p = nullptr;
+        const size_t want = (size_t)64 * (size_t)std::max(maxc, 1);
+        if (cudaMalloc(&p, sizeof(unsigned long long) * want) != cudaSuccess)
+            return nullptr;
+        if (d_agg_session) {
+            cudaDeviceSynchronize();
+            cudaFree(d_agg_session);
+        }
+        d_agg_session = p;
+        cap_agg_session = want;
+    }
+    return d_agg_session + (size_t)s * (size_t)std::max(maxc, 1);
+}
+}  // namespace pbrcm
+
+extern "C" {
+
+int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg, pbrcm_session** out)
+{
+    if (!ctx || !out)
+        return PBRCM_ERR_ARG;
+    *out = nullptr;
+    auto* s = new (std::nothrow) pbrcm_session();
+    if (!s)
+        return PBRCM_ERR_OOM;
+    s->C = &ctx->ctx;
+    cudaSetDevice(s->C->device);
+    s->cap_bytes = cfg && cfg->memory_cap_bytes ? cfg->memory_cap_bytes : 120ull * 1000 * 1000 * 1000;
+    s->max_inflight = cfg && cfg->max_inflight ? cfg->max_inflight : 4096;
+    const uint32_t ns = cfg && cfg->streams ? std::min<uint32_t>(cfg->streams, 64) : 8;
+    for (uint32_t i = 0; i < ns; ++i) {
+        cudaStream_t st;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+            delete s;
+            return PBRCM_ERR_CUDA;
+        }
+        s->streams.push_back(st);
+    }
+    s->small_variant = s->C->batch_variant;
+    const int maxc = team_max_ctas(s->C->team_variant, s->C->sms);
+    s->team_ctas = std::max(1, std::min(maxc, s->C->sms / 2));
+    if (cudaDeviceGetDefaultMemPool(&s->pool, s->C->device) != cudaSuccess) {
+        delete s;
+        return PBRCM_ERR_CUDA;
+    }
+    uint64_t thr = ~0ull;
+    cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    // the agg slots must exist before any team launch
+    if (!s->C->d_agg_session_slot((int)ns - 1)) {
+        delete s;
+        return PBRCM_ERR_OOM;
+    }
+    s->worker = std::thread([s] { s->run(); });
+    *out = s;
+    return PBRCM_OK;
+}
+
+void pbrcm_session_destroy(pbrcm_session* s)
+{
+    if (!s)
+        return;
+    pbrcm_session_drain(s);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable())
+        s->worker.join();
+    cudaSetDevice(s->C->device);
+    for (auto& kv : s->all) {
+        Request* r = kv.second;
+        if (r->ev)
+            cudaEventDestroy(r->ev);
+        s->pinned.put(r->host, r->host_cap);
+        delete r;
+    }
+    for (cudaStream_t st : s->streams) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    delete s;
+}
+
+int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const uint32_t* col_idx, uint32_t n,
+                             uint64_t nnz, const pbrcm_options* opts, uint64_t* ticket)
+{
+    if (!s || !row_ptr || (!col_idx && nnz) || !ticket || n == 0 || n == 0xFFFFFFFFu || nnz >= 0xFFFFFFFFull)
+        return PBRCM_ERR_ARG;
+    auto* r = new (std::nothrow) Request();
+    if (!r)
+        return PBRCM_ERR_OOM;
+    r->n = n;
+    r->nnz = nnz;
+    r->opt = make_options(opts, kModeFull);
+    r->opt.phantom = 0;
+    uint32_t maxdeg = 0;
+    for (uint32_t i = 0; i < n; ++i)
+        maxdeg = std::max(maxdeg, row_ptr[i + 1] - row_ptr[i]);
+    r->maxdeg = maxdeg;
+    const int emax_small = kVariants[s->small_variant].emax;
+    r->team = n > s->team_cutoff_n || maxdeg > (uint32_t)emax_small;
+    size_t offs[9];
+    r->dev_bytes = device_bytes(n, nnz, r->team && maxdeg > (uint32_t)kVariants[s->C->team_variant].emax, offs);
+    r->d_rp = offs[0];
+    r->d_ci = offs[1];
+    r->d_claim = offs[2];
+    r->d_rec = offs[3];
+    r->d_perm = offs[4];
+    r->d_res = offs[5];
+    r->d_gs = offs[6];
+    r->d_cnt = offs[7];
+    r->d_hub = offs[8];
+    if (r->dev_bytes > s->cap_bytes) {
+        delete r;
+        return PBRCM_ERR_BUSY;
+    }
+    size_t o = 0;
+    r->off_rp = o;
+    o = align16(o + 4 * ((size_t)n + 1));
+    r->off_ci = o;
+    o = align16(o + 4 * (size_t)nnz);
+    r->off_view = o;
+    o = align16(o + sizeof(MatrixView));
+    r->off_perm = o;
+    o = align16(o + 4 * (size_t)n);
+    r->off_res = o;
+    o = align16(o + sizeof(DevResult));
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        cudaSetDevice(s->C->device);
+        r->host = static_cast<unsigned char*>(s->pinned.get(o, r->host_cap));
+        if (!r->host || cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess) {
+            s->pinned.put(r->host, r->host_cap);
+            delete r;
+            return PBRCM_ERR_OOM;
+        }
+    }
+    std::memcpy(r->host + r->off_rp, row_ptr, 4 * ((size_t)n + 1));
+    if (nnz)
+        std::memcpy(r->host + r->off_ci, col_idx, 4 * (size_t)nnz);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->ticket = s->next_ticket++;
+        r->t_submit = Clock::now();
+        if (!s->have_first) {
+            s->t_first = r->t_submit;
+            s->have_first = true;
+        }
+        s->all[r->ticket] = r;
+        s->queued.push_back(r);
+        ++s->submitted;
+        *ticket = r->ticket;
+    }
+    s->cv_work.notify_all();
+    return PBRCM_OK;
+}
+
+int32_t pbrcm_session_poll(pbrcm_session* s, uint64_t ticket, uint32_t* perm_out, pbrcm_result* result,
+                           int32_t* done)
+{
+    if (!s || !done)
+        return PBRCM_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end())
+        return PBRCM_ERR_NOT_FOUND;
+    Request* r = it->second;
+    if (r->state != 2) {
+        *done = 0;
+        return PBRCM_OK;
+    }
+    *done = 1;
+    DevResult res;
+    std::memcpy(&res, r->host + r->off_res, sizeof(res));
+    if (perm_out && r->rc == PBRCM_OK)
+        std::memcpy(perm_out, r->host + r->off_perm, 4 * (size_t)r->n);
+    if (result) {
+        fill_result(res, r->opt, result);
+        result->total_ms = (float)std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+        result->device_ms = 0.f;
+    }
+    int32_t rc = r->rc;
+    cudaEventDestroy(r->ev);
+    s->pinned.put(r->host, r->host_cap);
+    s->all.erase(it);
+    delete r;
+    return rc;
+}
+
+int32_t pbrcm_session_drain(pbrcm_session* s)
+{
+    if (!s)
+        return PBRCM_ERR_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_done.wait(lk, [&] { return s->queued.empty() && s->running.empty(); });
+    return PBRCM_OK;
+}
+
+int32_t pbrcm_session_stats_get(pbrcm_session* s, pbrcm_session_stats* st)
+{
+    if (!s || !st)
+        return PBRCM_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    std::memset(st, 0, sizeof(*st));
+    st->submitted = s->submitted;
+    st->completed = s->completed;
+    st->bytes_in_flight = s->bytes_in_flight;
+    st->peak_bytes_in_flight = s->peak_bytes;
+    if (!s->lat_ms.empty()) {
+        std::vector<double> v = s->lat_ms;
+        std::sort(v.begin(), v.end());
+        auto q = [&](double f) { return v[std::min(v.size() - 1, (size_t)(f * (double)(v.size() - 1) + 0.5))]; };
+        st->p50_ms = q(0.50);
+        st->p99_ms = q(0.99);
+        st->max_ms = v.back();
+    }
+    if (s->have_first && s->completed)
+        st->busy_s = std::chrono::duration<double>(s->t_last - s->t_first).count();
+    return PBRCM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,431 @@
+"""Python host API over libpbrcm (the C ABI in include/pbrcm.h).
+
+Two layers:
+
+* array API -- ``reorder``, ``reorder_device``, ``find_peripheral``,
+  ``bandwidth``, ``reorder_batch``, ``Session``, ``load_mtx``,
+  ``prepare_csr``: numpy host arrays (or torch CUDA tensors for the device
+  forms) in, numpy / tensors out.
+* reference-shaped API -- ``Graph``, ``GPU_BATCH.rcm``,
+  ``SimplePeripheral.find_peripheral``, ``compute_bandwidth``,
+  ``check_bandwidth``, ``max_valency``, ``check_permutation``: the names,
+  argument meaning and error behaviour of the reference's GPU_BATCH surface
+  (include/rcm_gpu_batch.h:40-41, include/simple_peripheral.h:46,
+  src/main.cpp:94-226), so that code written against the reference reads the
+  same.
+
+Every call runs on the GPU through libpbrcm; a failing status raises
+``PbrcmError`` (the reference throws std::runtime_error on a device error,
+src/device/rcm_gpu_batch.cu:84-87).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import AUTO_START, DEBUG_PHANTOM_CTA, Matrix, Options, Result, SessionConfig, SessionStats
+
+__all__ = [
+    "PbrcmError", "Context", "default_options", "reorder", "reorder_device", "find_peripheral",
+    "bandwidth", "reorder_batch", "reorder_batch_device", "Session", "load_mtx", "prepare_csr",
+    "Graph", "GPU_BATCH", "SimplePeripheral", "compute_bandwidth", "check_bandwidth", "max_valency",
+    "check_permutation", "AUTO_START", "DEBUG_PHANTOM_CTA",
+]
+
+
+class PbrcmError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = int(status)
+        self.name = _lib.STATUS.get(self.status, str(status))
+        super().__init__(f"{what}: {self.name}" if what else self.name)
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise PbrcmError(rc, what)
+
+
+def _u32(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    return a
+
+
+def _ptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def default_options(reverse: bool = True, start: int | None = None, want_bandwidth: bool = True,
+                    peripheral_nodes: int = 32, wait_limit_ms: int = 2000, debug_flags: int = 0,
+                    stable: bool = True) -> Options:
+    o = Options()
+    _lib.lib().pbrcm_default_options(ctypes.byref(o))
+    o.reverse = 1 if reverse else 0
+    o.start_node = AUTO_START if start is None else int(start)
+    o.want_bandwidth = 1 if want_bandwidth else 0
+    o.peripheral_nodes = int(peripheral_nodes)
+    o.wait_limit_ms = int(wait_limit_ms)
+    o.debug_flags = int(debug_flags)
+    o.stable = 1 if stable else 0
+    return o
+
+
+class Context:
+    """A device context (stream + reusable device workspace)."""
+
+    def __init__(self, device: int = -1):
+        h = ctypes.c_void_p()
+        _check(_lib.lib().pbrcm_context_create(int(device), ctypes.byref(h)), "pbrcm_context_create")
+        self.handle = h
+
+    def close(self) -> None:
+        if self.handle:
+            _lib.lib().pbrcm_context_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _h(ctx):
+    return ctx.handle if ctx is not None else None
+
+
+def reorder(row_ptr, col_idx, *, reverse: bool = True, start: int | None = None, want_bandwidth: bool = True,
+            ctx: Context | None = None, perm_out: np.ndarray | None = None, raise_on_error: bool = True,
+            **opt_kw):
+    """Full reorder of one matrix from host arrays.  Returns (perm, result
+    dict); perm[k] = original node at position k (reversed CM when
+    `reverse`)."""
+    rp, ci = _u32(row_ptr), _u32(col_idx)
+    n = rp.shape[0] - 1
+    perm = perm_out if perm_out is not None else np.empty(max(n, 1), dtype=np.uint32)
+    res = Result()
+    o = default_options(reverse=reverse, start=start, want_bandwidth=want_bandwidth, **opt_kw)
+    rc = _lib.lib().pbrcm_reorder(_h(ctx), _ptr(rp), _ptr(ci), n, ci.shape[0], ctypes.byref(o), _ptr(perm),
+                                  ctypes.byref(res))
+    if raise_on_error:
+        _check(rc, "pbrcm_reorder")
+    d = res.as_dict()
+    d["rc"] = rc
+    return perm[:n], d
+
+
+def reorder_device(row_ptr_t, col_idx_t, perm_t=None, *, reverse: bool = True, start: int | None = None,
+                   want_bandwidth: bool = True, ctx: Context | None = None, stream=None, raise_on_error=True,
+                   **opt_kw):
+    """Full reorder of one matrix whose CSR is already on the GPU (torch
+    int32/uint32 CUDA tensors).  Returns (perm tensor, result dict)."""
+    import torch
+
+    n = row_ptr_t.numel() - 1
+    if perm_t is None:
+        perm_t = torch.empty(n, dtype=torch.int32, device=row_ptr_t.device)
+    res = Result()
+    o = default_options(reverse=reverse, start=start, want_bandwidth=want_bandwidth, **opt_kw)
+    st = ctypes.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+    rc = _lib.lib().pbrcm_reorder_device(_h(ctx), ctypes.c_void_p(row_ptr_t.data_ptr()),
+                                         ctypes.c_void_p(col_idx_t.data_ptr()), n, col_idx_t.numel(),
+                                         ctypes.byref(o), ctypes.c_void_p(perm_t.data_ptr()), ctypes.byref(res), st)
+    if raise_on_error:
+        _check(rc, "pbrcm_reorder_device")
+    d = res.as_dict()
+    d["rc"] = rc
+    return perm_t, d
+
+
+def find_peripheral(row_ptr, col_idx, ctx: Context | None = None):
+    """(start, passes, eccentricity) of the pseudo-peripheral search
+    (src/simple_peripheral.cpp:92-141) on the GPU."""
+    rp, ci = _u32(row_ptr), _u32(col_idx)
+    s, p, e = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    _check(_lib.lib().pbrcm_find_peripheral(_h(ctx), _ptr(rp), _ptr(ci), rp.shape[0] - 1, ci.shape[0],
+                                            ctypes.byref(s), ctypes.byref(p), ctypes.byref(e)),
+           "pbrcm_find_peripheral")
+    return s.value, p.value, e.value
+
+
+def bandwidth(row_ptr, col_idx, perm, ctx: Context | None = None):
+    """(bandwidth, initial_bandwidth, profile) of `perm` on the GPU."""
+    rp, ci, pm = _u32(row_ptr), _u32(col_idx), _u32(perm)
+    bw, bw0, prof = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_uint64()
+    _check(_lib.lib().pbrcm_bandwidth(_h(ctx), _ptr(rp), _ptr(ci), rp.shape[0] - 1, ci.shape[0], _ptr(pm),
+                                      ctypes.byref(bw), ctypes.byref(bw0), ctypes.byref(prof)), "pbrcm_bandwidth")
+    return bw.value, bw0.value, prof.value
+
+
+def reorder_batch(mats: Sequence, *, reverse: bool = True, start: int | None = None, want_bandwidth: bool = True,
+                  ctx: Context | None = None, raise_on_error: bool = True, **opt_kw):
+    """Reorders many (row_ptr, col_idx) host matrices in one persistent
+    launch.  Returns (list of perms, list of result dicts)."""
+    keep = []
+    arr = (Matrix * len(mats))()
+    perms = []
+    for i, m in enumerate(mats):
+        rp, ci = _u32(m[0]), _u32(m[1])
+        n = rp.shape[0] - 1
+        p = np.empty(max(n, 1), dtype=np.uint32)
+        keep += [rp, ci]
+        perms.append(p)
+        arr[i].row_ptr = rp.ctypes.data
+        arr[i].col_idx = ci.ctypes.data
+        arr[i].n = n
+        arr[i].nnz = ci.shape[0]
+        arr[i].perm_out = p.ctypes.data
+    res = (Result * len(mats))()
+    o = default_options(reverse=reverse, start=start, want_bandwidth=want_bandwidth, **opt_kw)
+    rc = _lib.lib().pbrcm_reorder_batch(_h(ctx), arr, len(mats), ctypes.byref(o), res)
+    if raise_on_error:
+        _check(rc, "pbrcm_reorder_batch")
+    out = [r.as_dict() for r in res]
+    return [p[: (np.asarray(m[0]).shape[0] - 1)] for p, m in zip(perms, mats)], out
+
+
+def reorder_batch_device(mats: Sequence, *, reverse: bool = True, ctx: Context | None = None, stream=None,
+                         raise_on_error: bool = True, **opt_kw):
+    """Batched reorder of device-resident (row_ptr, col_idx, perm_out) torch
+    tensors.  Returns the result dicts."""
+    import torch
+
+    arr = (Matrix * len(mats))()
+    for i, (rp, ci, po) in enumerate(mats):
+        arr[i].row_ptr = rp.data_ptr()
+        arr[i].col_idx = ci.data_ptr()
+        arr[i].n = rp.numel() - 1
+        arr[i].nnz = ci.numel()
+        arr[i].perm_out = po.data_ptr()
+    res = (Result * len(mats))()
+    o = default_options(reverse=reverse, **opt_kw)
+    st = ctypes.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+    rc = _lib.lib().pbrcm_reorder_batch_device(_h(ctx), arr, len(mats), ctypes.byref(o), res, st)
+    if raise_on_error:
+        _check(rc, "pbrcm_reorder_batch_device")
+    return [r.as_dict() for r in res]
+
+
+class Session:
+    """Serving session: submit requests at any time; they are admitted by
+    device memory footprint and run concurrently (continuous batching)."""
+
+    def __init__(self, ctx: Context, memory_cap_bytes: int = 0, max_inflight: int = 0, streams: int = 0):
+        cfg = SessionConfig()
+        cfg.memory_cap_bytes = memory_cap_bytes
+        cfg.max_inflight = max_inflight
+        cfg.streams = streams
+        h = ctypes.c_void_p()
+        _check(_lib.lib().pbrcm_session_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(h)),
+               "pbrcm_session_create")
+        self.handle = h
+        self.ctx = ctx
+        self._n = {}
+
+    def submit(self, row_ptr, col_idx, *, reverse: bool = True, start: int | None = None,
+               want_bandwidth: bool = True, **opt_kw) -> int:
+        rp, ci = _u32(row_ptr), _u32(col_idx)
+        t = ctypes.c_uint64()
+        o = default_options(reverse=reverse, start=start, want_bandwidth=want_bandwidth, **opt_kw)
+        _check(_lib.lib().pbrcm_session_submit(self.handle, _ptr(rp), _ptr(ci), rp.shape[0] - 1, ci.shape[0],
+                                               ctypes.byref(o), ctypes.byref(t)), "pbrcm_session_submit")
+        self._n[t.value] = rp.shape[0] - 1
+        return t.value
+
+    def poll(self, ticket: int):
+        """None while running; (perm, result dict) once done."""
+        n = self._n[ticket]
+        perm = np.empty(max(n, 1), dtype=np.uint32)
+        res = Result()
+        done = ctypes.c_int32()
+        rc = _lib.lib().pbrcm_session_poll(self.handle, ticket, _ptr(perm), ctypes.byref(res), ctypes.byref(done))
+        if rc != 0 and done.value == 0:
+            _check(rc, "pbrcm_session_poll")
+        if not done.value:
+            return None
+        del self._n[ticket]
+        d = res.as_dict()
+        d["rc"] = rc
+        return perm[:n], d
+
+    def drain(self) -> None:
+        _check(_lib.lib().pbrcm_session_drain(self.handle), "pbrcm_session_drain")
+
+    def stats(self) -> dict:
+        st = SessionStats()
+        _check(_lib.lib().pbrcm_session_stats_get(self.handle, ctypes.byref(st)), "pbrcm_session_stats_get")
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def close(self) -> None:
+        if self.handle:
+            _lib.lib().pbrcm_session_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def _take_csr(n: int, nnz: int, rp_p, ci_p):
+    L = _lib.lib()
+    rp = np.ctypeslib.as_array(rp_p, shape=(n + 1,)).copy()
+    ci = np.ctypeslib.as_array(ci_p, shape=(max(nnz, 1),))[:nnz].copy()
+    L.pbrcm_free(ctypes.cast(rp_p, ctypes.c_void_p))
+    L.pbrcm_free(ctypes.cast(ci_p, ctypes.c_void_p))
+    return rp, ci
+
+
+def load_mtx(path: str):
+    """(row_ptr, col_idx) of a MatrixMarket file with the reference loader's
+    semantics (include/Graph.h:266-332), without writing cache files."""
+    n, nnz = ctypes.c_uint32(), ctypes.c_uint64()
+    rp_p, ci_p = ctypes.POINTER(ctypes.c_uint32)(), ctypes.POINTER(ctypes.c_uint32)()
+    _check(_lib.lib().pbrcm_load_mtx(path.encode(), ctypes.byref(n), ctypes.byref(nnz), ctypes.byref(rp_p),
+                                     ctypes.byref(ci_p)), f"pbrcm_load_mtx({path})")
+    return _take_csr(n.value, nnz.value, rp_p, ci_p)
+
+
+def prepare_csr(row_ptr, col_idx, check_symmetry: bool = True):
+    """prepareRCM (include/Graph.h:74-264): symmetry repair + connectivity
+    repair of a raw CSR."""
+    rp, ci = _u32(row_ptr), _u32(col_idx)
+    nnz = ctypes.c_uint64()
+    rp_p, ci_p = ctypes.POINTER(ctypes.c_uint32)(), ctypes.POINTER(ctypes.c_uint32)()
+    _check(_lib.lib().pbrcm_prepare_csr(_ptr(rp), _ptr(ci), rp.shape[0] - 1, ci.shape[0], int(check_symmetry),
+                                        ctypes.byref(nnz), ctypes.byref(rp_p), ctypes.byref(ci_p)),
+           "pbrcm_prepare_csr")
+    return _take_csr(rp.shape[0] - 1, nnz.value, rp_p, ci_p)
+
+
+# ---------------------------------------------------------------------------
+# Reference-shaped surface
+# ---------------------------------------------------------------------------
+
+@dataclass
+class _CSR:
+    """Mirror of CSR<T> (include/CSR.h:43-75): rows, cols, nnz, row_offsets,
+    col_ids, data."""
+    row_offsets: np.ndarray
+    col_ids: np.ndarray
+    data: np.ndarray | None = None
+
+    @property
+    def rows(self) -> int:
+        return int(self.row_offsets.shape[0] - 1)
+
+    @property
+    def cols(self) -> int:
+        return self.rows
+
+    @property
+    def nnz(self) -> int:
+        return int(self.col_ids.shape[0])
+
+
+@dataclass
+class Graph:
+    """Mirror of Graph<T> (include/Graph.h:42-333)."""
+    csr: _CSR = field(default_factory=lambda: _CSR(np.zeros(1, np.uint32), np.zeros(0, np.uint32)))
+
+    @classmethod
+    def from_csr(cls, row_offsets, col_ids) -> "Graph":
+        return cls(_CSR(_u32(row_offsets), _u32(col_ids)))
+
+    def load(self, file: str) -> int:
+        """Graph::load (include/Graph.h:266-332): 0 on success, -1 if the file
+        cannot be read (the reference prints the error and returns -1)."""
+        try:
+            rp, ci = load_mtx(file)
+        except PbrcmError:
+            return -1
+        self.csr = _CSR(rp, ci)
+        return 0
+
+    @property
+    def size(self) -> int:
+        return self.csr.rows
+
+    def neighbour_count(self, node: int) -> int:
+        return int(self.csr.row_offsets[node + 1] - self.csr.row_offsets[node])
+
+    def prepareRCM(self, check_sym: bool = True) -> None:
+        rp, ci = prepare_csr(self.csr.row_offsets, self.csr.col_ids, check_sym)
+        self.csr = _CSR(rp, ci)
+
+
+class GPU_BATCH:
+    """Mirror of namespace GPU_BATCH (include/rcm_gpu_batch.h:37-45)."""
+
+    @staticmethod
+    def rcm(graph: Graph, csv_file, permutation: list, start_node: int, ctx: Context | None = None) -> None:
+        """GPU_BATCH::rcm (src/device/rcm_gpu_batch.cu:42-112): fills
+        `permutation` with the Cuthill-McKee order from `start_node` (the
+        reference's output order: not reversed) and appends the device time in
+        ms to `csv_file` (any object with write(), or None)."""
+        perm, res = reorder(graph.csr.row_offsets, graph.csr.col_ids, reverse=False, start=start_node,
+                            want_bandwidth=False, ctx=ctx)
+        permutation.clear()
+        permutation.extend(int(x) for x in perm)
+        if csv_file is not None:
+            csv_file.write(f"{res['device_ms']}")
+
+    @staticmethod
+    def findPeripheral(graph: Graph, csv_file=None, writeOutput: bool = False, ctx: Context | None = None) -> int:
+        return SimplePeripheral.findPeripheral(graph, csv_file, writeOutput, ctx=ctx)
+
+
+class SimplePeripheral:
+    """Mirror of namespace SimplePeripheral (include/simple_peripheral.h:40-47),
+    computed on the GPU."""
+
+    @staticmethod
+    def findPeripheral(graph: Graph, csv_file=None, writeOutput: bool = False, outputnodes: int = 32,
+                       ctx: Context | None = None) -> int:
+        if outputnodes != 32:
+            raise ValueError("the GPU search keeps 32 nodes per pass, as the reference default")
+        s, _, _ = find_peripheral(graph.csr.row_offsets, graph.csr.col_ids, ctx=ctx)
+        return s
+
+
+def compute_bandwidth(graph: Graph, permutation: Iterable[int]) -> int:
+    """computeBandwidth (src/main.cpp:143-184); -1 for an empty permutation."""
+    perm = _u32(list(permutation) if not isinstance(permutation, np.ndarray) else permutation)
+    if perm.shape[0] == 0:
+        return -1
+    bw, _, _ = bandwidth(graph.csr.row_offsets, graph.csr.col_ids, perm)
+    return int(bw)
+
+
+def check_bandwidth(graph: Graph) -> int:
+    """checkBandwidth (src/main.cpp:114-129): bandwidth of the input as
+    stored."""
+    n = graph.csr.rows
+    _, bw0, _ = bandwidth(graph.csr.row_offsets, graph.csr.col_ids, np.arange(n, dtype=np.uint32))
+    return int(bw0)
+
+
+def max_valency(graph: Graph) -> int:
+    """maxValency (src/main.cpp:131-140)."""
+    return int(np.max(np.diff(graph.csr.row_offsets.astype(np.int64)))) if graph.csr.rows else 0
+
+
+def check_permutation(permutation) -> int:
+    """checkPermutation (src/main.cpp:186-226): 0 if a bijection, -1 if not."""
+    p = np.asarray(permutation, dtype=np.int64)
+    n = p.shape[0]
+    if n == 0:
+        return 0
+    if p.min() < 0 or p.max() >= n:
+        return -1
+    return 0 if np.unique(p).shape[0] == n else -1
