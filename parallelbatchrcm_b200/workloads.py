@@ -1,0 +1,261 @@
+"""Many-matrix and serving benchmarks (``bench.py --workload batch|serve``).
+
+batch  4096 independent matrices, n log-uniform in [500, 200000]: 40% 2-D
+       grids, 30% 3-D grids, 30% RGGs with k ~ U{4..12} (seed 42).  Measures
+       the one-launch batched engine (pbrcm_reorder_batch_device, CSRs resident
+       in HBM) against plain one-matrix-at-a-time GPU RCM (one team launch per
+       matrix, pbrcm_reorder_device, same engine), checks that every batched
+       permutation equals the one-at-a-time one, and samples matrices against
+       the oracle.
+serve  Poisson arrivals of requests with n log-uniform in [1000, 2000000]
+       over the three generators (seed 99).  The serving session (continuous
+       batching) against a plain FIFO worker that reorders one request at a
+       time with pbrcm_reorder; both start from host buffers.  Reports
+       throughput and p50/p99 latency (arrival -> result) per arrival rate.
+"""
+from __future__ import annotations
+
+import json
+import multiprocessing as mp
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+from . import gen
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def _make(spec):
+    m = gen.make_from_spec(spec)
+    return m.row_ptr, m.col_idx
+
+
+def generate(specs, procs: int | None = None):
+    """Generates the matrices of `specs` with a spawn-started process pool
+    (started before any CUDA call)."""
+    procs = procs or max(1, min(len(specs), (os.cpu_count() or 2) - 1, 64))
+    if procs == 1 or len(specs) < 8:
+        return [_make(s) for s in specs]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        return pool.map(_make, specs, chunksize=max(1, len(specs) // (procs * 8)))
+
+
+def _quantiles(v):
+    v = sorted(v)
+    if not v:
+        return None, None
+    q = lambda f: v[min(len(v) - 1, int(round(f * (len(v) - 1))))]  # noqa: E731
+    return q(0.5), q(0.99)
+
+
+def run_batch(args, ws, rank, local):
+    import torch
+
+    import parallelbatchrcm_b200 as P
+
+    count = int(os.environ.get("PBRCM_BATCH_COUNT", "4096"))
+    t0 = time.time()
+    specs = gen.mixed_batch_specs(count=count, seed=42)
+    mats = generate(specs)
+    sum_n = sum(int(rp.shape[0] - 1) for rp, _ in mats)
+    sum_nnz = sum(int(ci.shape[0]) for _, ci in mats)
+    log(f"generated {count} matrices: sum n={sum_n} sum nnz={sum_nnz} in {time.time() - t0:.1f}s")
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ctx = P.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    dmats = []
+    for rp, ci in mats:
+        dmats.append((torch.from_numpy(rp.view(np.int32)).to(dev), torch.from_numpy(ci.view(np.int32)).to(dev),
+                      torch.empty(rp.shape[0] - 1, dtype=torch.int32, device=dev)))
+    torch.cuda.synchronize()
+
+    def batched():
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        res = P.reorder_batch_device(dmats, reverse=True, ctx=ctx, stream=stream)
+        ev1.record(stream)
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1), res
+
+    for _ in range(args.warmup):
+        batched()
+    times = []
+    for _ in range(args.steps):
+        ms, res = batched()
+        times.append(ms)
+    assert all(r["status"] == 0 for r in res), [r for r in res if r["status"] != 0][:3]
+    bperm = [p.cpu().numpy().copy() for _, _, p in dmats]
+    batch_ms = statistics.median(times)
+
+    # plain one-at-a-time: one team launch per matrix, same stream
+    plain_perm = []
+    tplain = 0.0
+    lat = []
+    for rp_d, ci_d, po in dmats:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        P.reorder_device(rp_d, ci_d, po, reverse=True, ctx=ctx, stream=stream)
+        ev1.record(stream)
+        ev1.synchronize()
+        lat.append(ev0.elapsed_time(ev1))
+        tplain += lat[-1]
+        plain_perm.append(po.cpu().numpy().copy())
+    same = all(np.array_equal(a, b) for a, b in zip(bperm, plain_perm))
+
+    # oracle sample
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import oracle as O
+    rng = np.random.default_rng(0)
+    sample = rng.choice(count, size=min(64, count), replace=False)
+    oracle_ok = all(np.array_equal(bperm[i].view(np.uint32),
+                                   O.full_reorder(mats[i][0], mats[i][1], reverse=True)["perm"]) for i in sample)
+
+    # e2e from pinned host buffers through pbrcm_reorder_batch
+    hm = [(torch.from_numpy(rp.view(np.int32)).pin_memory().numpy().view(np.uint32),
+           torch.from_numpy(ci.view(np.int32)).pin_memory().numpy().view(np.uint32)) for rp, ci in mats]
+    P.reorder_batch(hm, reverse=True, ctx=ctx)
+    e2e = []
+    for _ in range(max(1, args.steps // 2)):
+        t1 = time.perf_counter()
+        P.reorder_batch(hm, reverse=True, ctx=ctx)
+        e2e.append(time.perf_counter() - t1)
+    e2e_s = statistics.median(e2e)
+
+    value = count / (batch_ms / 1e3)
+    plain_value = count / (tplain / 1e3)
+    line = {
+        "metric": "reorders/s (batched, many matrices, one persistent launch)", "value": value,
+        "unit": "reorders/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": batch_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic (seeded mixed grids / RGGs)",
+        "config": {"workload": f"mixed_batch_{count}", "sum_n": sum_n, "sum_nnz": sum_nnz,
+                   "l2": "inputs (GBs) larger than L2"},
+        "gnnz_per_s": sum_nnz / (batch_ms / 1e3) / 1e9,
+        "plain_one_at_a_time": {"value": plain_value, "unit": "reorders/s", "total_ms": tplain,
+                                "p50_ms": _quantiles(lat)[0], "p99_ms": _quantiles(lat)[1]},
+        "speedup_vs_plain": value / plain_value,
+        "batched_equals_plain": bool(same), "oracle_sample_ok": bool(oracle_ok), "oracle_sample": int(len(sample)),
+        "e2e": {"value": count / e2e_s, "unit": "reorders/s",
+                "h2d_bytes_per_step": int(sum(4 * (rp.shape[0] + ci.shape[0]) for rp, ci in mats)),
+                "d2h_bytes_per_step": int(4 * sum_n)},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _serve_session(ctx, mats, arrivals, streams):
+    import parallelbatchrcm_b200 as P
+
+    sess = P.Session(ctx, streams=streams)
+    n = len(mats)
+    tick = [None] * n
+    t_sub = [0.0] * n
+    done_at = [None] * n
+    t0 = time.perf_counter() + 0.05
+
+    def submitter():
+        for i in range(n):
+            while True:
+                d = t0 + arrivals[i] - time.perf_counter()
+                if d <= 0:
+                    break
+                time.sleep(min(d, 0.001))
+            t_sub[i] = time.perf_counter()
+            tick[i] = sess.submit(mats[i][0], mats[i][1])
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    pending = set(range(n))
+    while pending:
+        for i in list(pending):
+            if tick[i] is None:
+                continue
+            out = sess.poll(tick[i])
+            if out is not None:
+                done_at[i] = time.perf_counter()
+                assert out[1]["status"] == 0
+                pending.discard(i)
+        time.sleep(0.0002)
+    th.join()
+    lat = [(done_at[i] - (t0 + arrivals[i])) * 1e3 for i in range(n)]
+    makespan = max(done_at) - t0
+    sess.close()
+    return lat, makespan
+
+
+def _serve_plain(ctx, mats, arrivals):
+    import parallelbatchrcm_b200 as P
+
+    n = len(mats)
+    done_at = [0.0] * n
+    t0 = time.perf_counter() + 0.05
+    for i in range(n):
+        d = t0 + arrivals[i] - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        P.reorder(mats[i][0], mats[i][1], ctx=ctx)
+        done_at[i] = time.perf_counter()
+    lat = [(done_at[i] - (t0 + arrivals[i])) * 1e3 for i in range(n)]
+    return lat, max(done_at) - t0
+
+
+def run_serve(args, ws, rank, local):
+    import torch
+
+    import parallelbatchrcm_b200 as P
+
+    count = int(os.environ.get("PBRCM_SERVE_COUNT", "256"))
+    rates = [float(x) for x in os.environ.get("PBRCM_SERVE_RATES", "50,200,1000,100000").split(",")]
+    stream_specs = gen.poisson_stream_specs(count, rate_per_s=1.0, seed=99)
+    gaps = np.array([t for t, _ in stream_specs])  # arrival times at rate 1/s
+    t0 = time.time()
+    mats = generate([s for _, s in stream_specs])
+    mats = [(rp, ci) for rp, ci in mats]
+    log(f"generated {count} requests: sum n={sum(r.shape[0] - 1 for r, _ in mats)} in {time.time() - t0:.1f}s")
+    torch.cuda.set_device(local)
+    ctx = P.Context(local)
+    # warm-up both paths
+    _serve_session(ctx, mats[:16], [0.0] * 16, 8)
+    for rp, ci in mats[:4]:
+        P.reorder(rp, ci, ctx=ctx)
+    rows = []
+    for rate in rates:
+        arr = list(gaps / rate)
+        lat_s, span_s = _serve_session(ctx, mats, arr, 16)
+        lat_p, span_p = _serve_plain(ctx, mats, arr)
+        r = {"rate_per_s": rate,
+             "session": {"reorders_per_s": count / span_s, "p50_ms": _quantiles(lat_s)[0],
+                         "p99_ms": _quantiles(lat_s)[1]},
+             "plain": {"reorders_per_s": count / span_p, "p50_ms": _quantiles(lat_p)[0],
+                       "p99_ms": _quantiles(lat_p)[1]}}
+        log(json.dumps(r))
+        rows.append(r)
+    best = rows[-1]
+    line = {
+        "metric": "reorders/s (serving, continuous batching, Poisson arrivals)",
+        "value": best["session"]["reorders_per_s"], "unit": "reorders/s", "n_gpus": ws, "steps": len(rates),
+        "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded Poisson stream of grids / RGGs, n in [1e3, 2e6])",
+        "config": {"workload": f"serve_poisson_{count}", "rates": rates, "admission_cap_gb": 120},
+        "sweep": rows,
+        "speedup_vs_plain_at_max_rate": best["session"]["reorders_per_s"] / best["plain"]["reorders_per_s"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(args, ws, rank, local):
+    if args.workload == "batch":
+        return run_batch(args, ws, rank, local)
+    if args.workload == "serve":
+        return run_serve(args, ws, rank, local)
+    raise ValueError(args.workload)
