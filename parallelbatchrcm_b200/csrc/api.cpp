@@ -50,7 +50,16 @@ Options make_options(const pbrcm_options* o, uint32_t mode)
     opt.wait_ns = (unsigned long long)(o->wait_limit_ms ? o->wait_limit_ms : 2000u) * 1000000ull;
     opt.phantom = (o->debug_flags & PBRCM_DEBUG_PHANTOM_CTA) ? 1u : 0u;
     opt.mode = mode;
+    opt.solo_edges = 0;
+    opt.solo_parents = 0;
     return opt;
+}
+
+void apply_team_shape(const Context& C, Options& opt)
+{
+    opt.solo_edges = C.solo_edges;
+    opt.solo_parents = C.solo_parents;
+    opt.barrier = C.barrier;
 }
 
 void fill_result(const DevResult& r, const Options& opt, pbrcm_result* out)
@@ -107,19 +116,24 @@ int32_t Context::init(int dev)
     if (cudaMallocHost(&h_res, sizeof(DevResult)) != cudaSuccess)
         return PBRCM_ERR_OOM;
     // team shape: variant and CTA count (PBRCM_TEAM_VARIANT / PBRCM_TEAM_CTAS override)
-    team_variant = env_int("PBRCM_TEAM_VARIANT", 2);
+    team_variant = env_int("PBRCM_TEAM_VARIANT", 1);
     if (team_variant < 0 || team_variant >= kNumVariants)
-        team_variant = 2;
+        team_variant = 1;
     int maxc = team_max_ctas(team_variant, sms);
     if (maxc <= 0)
         return PBRCM_ERR_CUDA;
+    team_maxc = maxc;
     team_ctas = env_int("PBRCM_TEAM_CTAS", 0);
     if (team_ctas <= 0 || team_ctas > maxc)
         team_ctas = std::min(maxc, sms);
-    batch_variant = env_int("PBRCM_BATCH_VARIANT", 1);
+    // levels of at most 2 chunks run on CTA 0 alone
+    solo_parents = (uint32_t)env_int("PBRCM_SOLO_PARENTS", 2 * kVariants[team_variant].block);
+    solo_edges = (uint32_t)env_int("PBRCM_SOLO_EDGES", 2 * kVariants[team_variant].emax);
+    barrier = (uint32_t)env_int("PBRCM_BARRIER", 0) ? 1u : 0u;
+    batch_variant = env_int("PBRCM_BATCH_VARIANT", 2);
     if (batch_variant < 0 || batch_variant >= kNumVariants)
-        batch_variant = 1;
-    if (cudaMalloc(&d_agg, sizeof(unsigned long long) * (size_t)std::max(maxc, 1)) != cudaSuccess)
+        batch_variant = 2;
+    if (cudaMalloc(&d_agg, team_words_bytes(maxc)) != cudaSuccess)
         return PBRCM_ERR_OOM;
     return PBRCM_OK;
 }
@@ -130,9 +144,9 @@ Context::~Context()
         cudaSetDevice(device);
     if (stream)
         cudaStreamSynchronize(stream);
-    for (void* p : {(void*)d_rp, (void*)d_ci, (void*)d_claim, (void*)d_perm, (void*)d_rec, (void*)d_hub,
-                    (void*)d_res, (void*)d_gs, (void*)d_agg, (void*)d_jobs, (void*)d_counter, (void*)d_bres,
-                    (void*)d_arena, (void*)d_agg_session})
+    for (void* p : {(void*)d_rp, (void*)d_ci, (void*)d_node, (void*)d_perm, (void*)d_rec, (void*)d_hub,
+                    (void*)d_res, (void*)d_gs, (void*)d_agg, (void*)d_jobs, (void*)d_slots, (void*)d_counter, (void*)d_bres,
+                    (void*)d_arena})
         if (p)
             cudaFree(p);
     if (h_res)
@@ -167,7 +181,7 @@ bool Context::ensure_single(uint32_t n, uint64_t nnz, bool inputs)
 {
     if (inputs && (!grow(d_rp, cap_rp, (size_t)n + 1) || !grow(d_ci, cap_ci, (size_t)nnz)))
         return false;
-    return grow(d_claim, cap_claim, n) && grow(d_rec, cap_rec, n) && grow(d_perm, cap_perm, n);
+    return grow(d_node, cap_node, n) && grow(d_rec, cap_rec, n) && grow(d_perm, cap_perm, n);
 }
 
 bool Context::ensure_hub(uint64_t nnz) { return grow(d_hub, cap_hub, 4 * (size_t)std::max<uint64_t>(nnz, 1)); }
@@ -184,18 +198,21 @@ int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
         M.ci = ci;
         M.n = n;
         M.nnz = (uint32_t)nnz;
-        M.claim = d_claim;
+        M.node = d_node;
         M.rec = d_rec;
         M.perm = perm;
         M.hub = with_hub ? d_hub : nullptr;
         M.res = d_res;
         if (cudaMemsetAsync(d_res, 0, sizeof(DevResult), st) != cudaSuccess ||
-            cudaMemsetAsync(d_gs, 0, sizeof(GridSync), st) != cudaSuccess)
+            cudaMemsetAsync(d_gs, 0, sizeof(GridSync), st) != cudaSuccess ||
+            cudaMemsetAsync(d_agg, 0, team_words_bytes(team_ctas), st) != cudaSuccess)
             return PBRCM_ERR_CUDA;
         if (launch_validate(rp, ci, n, (uint32_t)nnz, d_res, sms, st) != cudaSuccess)
             return PBRCM_ERR_CUDA;
         cudaEventRecord(ev0, st);
-        cudaError_t e = launch_team(team_variant, M, opt, d_gs, d_agg, team_ctas, st);
+        Options o = opt;
+        apply_team_shape(*this, o);
+        cudaError_t e = launch_team(team_variant, M, o, d_gs, d_agg, team_ctas, st);
         cudaEventRecord(ev1, st);
         if (e != cudaSuccess)
             return PBRCM_ERR_CUDA;
@@ -219,7 +236,7 @@ int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
 
 static int32_t check_sizes(uint32_t n, uint64_t nnz)
 {
-    if (n == 0 || n == 0xFFFFFFFFu || nnz >= 0xFFFFFFFFull)
+    if (n == 0 || n == 0xFFFFFFFFu || nnz > kMaxNnz)
         return PBRCM_ERR_ARG;
     return PBRCM_OK;
 }
@@ -434,7 +451,8 @@ int32_t pbrcm_bandwidth(pbrcm_context* ctx, const uint32_t* row_ptr, const uint3
         cudaMemsetAsync(C.d_res, 0, sizeof(DevResult), st) != cudaSuccess)
         return PBRCM_ERR_CUDA;
     if (launch_validate(C.d_rp, C.d_ci, n, (uint32_t)nnz, C.d_res, C.sms, st) != cudaSuccess ||
-        launch_bandwidth(C.d_rp, C.d_ci, n, C.d_perm, C.d_claim, C.d_res, C.sms, st) != cudaSuccess ||
+        launch_bandwidth(C.d_rp, C.d_ci, n, C.d_perm, reinterpret_cast<uint32_t*>(C.d_node), C.d_res, C.sms, st) !=
+            cudaSuccess ||
         cudaMemcpyAsync(C.h_res, C.d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return PBRCM_ERR_CUDA;

@@ -2,12 +2,14 @@
 // (pbrcm_reorder_batch / pbrcm_reorder_batch_device).
 //
 // Layout: one device arena per call holds, per matrix, its CSR (host-input
-// form only), claim[n], rec[n] and perm[n], each 16-byte aligned.  A job
-// table of MatrixView descriptors, sorted by nnz descending so that the
-// biggest matrices start first, drives k_reorder_batch: every CTA takes the
-// next job from an atomic counter and runs the whole reorder of that matrix
-// (start search, CM pass, reverse, bandwidth) with a one-CTA team.  Matrices
-// above the team cutoff run first, one cooperative team launch each.
+// form only), its node table node[n], rec[n] and perm[n] (host-input form
+// only), each 16-byte aligned.  Jobs are ordered by nnz, biggest first; a
+// job above the team threshold gets a team of K CTAs (K grows with its nnz)
+// with its own zeroed barrier words, the others one CTA.  The work list
+// holds K consecutive slots per job; k_reorder_batch (a cooperative launch,
+// so that every CTA is resident and a team always fills up) hands the slots
+// out with an atomic counter.  Every CTA of a job runs the whole reorder of
+// that matrix (start search, CM pass, reverse, bandwidth).
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -26,9 +28,10 @@ using namespace pbrcm;
 namespace {
 
 inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+inline size_t align128(size_t x) { return (x + 127) & ~(size_t)127; }
 
 struct Slot {
-    size_t rp, ci, claim, rec, perm;  // arena offsets (rp/ci unused for device input)
+    size_t rp, ci, node, rec, perm;  // arena offsets (rp/ci/perm unused for device input)
 };
 
 int env_int(const char* name, int dflt)
@@ -37,17 +40,68 @@ int env_int(const char* name, int dflt)
     return v && *v ? std::atoi(v) : dflt;
 }
 
+template <typename T>
+bool grow_dev(T*& p, size_t& cap, size_t need)
+{
+    if (need <= cap && p)
+        return true;
+    if (p)
+        cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMalloc(&p, sizeof(T) * std::max<size_t>(need, 1)) != cudaSuccess)
+        return false;
+    cap = std::max<size_t>(need, 1);
+    return true;
+}
+
+// Team size of a job: one CTA up to min_nnz entries, then one CTA per
+// nnz_per_cta entries, at most max_team.
+uint32_t team_size(uint64_t nnz, uint64_t min_nnz, uint64_t nnz_per_cta, uint32_t max_team)
+{
+    if (nnz < min_nnz || max_team < 2)
+        return 1;
+    const uint64_t k = (nnz + nnz_per_cta - 1) / nnz_per_cta;
+    return (uint32_t)std::max<uint64_t>(2, std::min<uint64_t>(k, max_team));
+}
+
 // Shared driver; `host` selects whether mats[] point to host or device memory.
 int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pbrcm_options* opts,
                   pbrcm_result* results, cudaStream_t st, bool host)
 {
     auto t0 = std::chrono::steady_clock::now();
     Options opt = make_options(opts, kModeFull);
+    const int v = C.batch_variant;
+    opt.solo_parents = 2 * kVariants[v].block;
+    opt.solo_edges = 2 * kVariants[v].emax;
+    opt.barrier = 0;
     for (uint32_t j = 0; j < count; ++j) {
         const pbrcm_matrix& m = mats[j];
         if (!m.row_ptr || (!m.col_idx && m.nnz) || !m.perm_out || m.n == 0 || m.n == 0xFFFFFFFFu ||
-            m.nnz >= 0xFFFFFFFFull)
+            m.nnz > kMaxNnz)
             return PBRCM_ERR_ARG;
+    }
+    const int maxc = batch_max_ctas(v, C.sms);
+    if (maxc <= 0)
+        return PBRCM_ERR_CUDA;
+    // job order (biggest first) and team sizes
+    const uint64_t min_nnz = (uint64_t)env_int("PBRCM_BATCH_TEAM_MIN_NNZ", 1 << 19);
+    const uint64_t per_cta = (uint64_t)std::max(1, env_int("PBRCM_BATCH_TEAM_NNZ", 1 << 18));
+    // teams are off by default: on mixed batches the total work, not the
+    // biggest matrix, bounds the makespan, and team members of a matrix whose
+    // levels are small idle at the gate (PBRCM_BATCH_TEAM_MAX enables them)
+    const uint32_t max_team = (uint32_t)std::max(1, std::min(env_int("PBRCM_BATCH_TEAM_MAX", 1), maxc));
+    std::vector<uint32_t> order(count);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return mats[a].nnz > mats[b].nnz; });
+    std::vector<uint32_t> team(count);
+    size_t nslots = 0, teamws = 0;
+    for (uint32_t q = 0; q < count; ++q) {
+        team[q] = team_size(mats[order[q]].nnz, min_nnz, per_cta, max_team);
+        nslots += team[q];
+        if (team[q] > 1)
+            teamws = align128(teamws + sizeof(GridSync)) + align128(team_words_bytes((int)team[q]));
     }
     // arena layout
     std::vector<Slot> slot(count);
@@ -60,8 +114,8 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
             slot[j].ci = off;
             off = align16(off + 4 * (size_t)m.nnz);
         }
-        slot[j].claim = off;
-        off = align16(off + 4 * (size_t)m.n);
+        slot[j].node = off;
+        off = align16(off + 16 * (size_t)m.n);
         slot[j].rec = off;
         off = align16(off + 16 * (size_t)m.n);
         if (host) {
@@ -69,34 +123,12 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
             off = align16(off + 4 * (size_t)m.n);
         }
     }
-    if (off > C.cap_arena) {
-        if (C.d_arena)
-            cudaFree(C.d_arena);
-        C.d_arena = nullptr;
-        C.cap_arena = 0;
-        if (cudaMalloc(&C.d_arena, off) != cudaSuccess)
-            return PBRCM_ERR_OOM;
-        C.cap_arena = off;
-    }
-    if (count > C.cap_jobs) {
-        if (C.d_jobs)
-            cudaFree(C.d_jobs);
-        if (C.d_bres)
-            cudaFree(C.d_bres);
-        C.d_jobs = nullptr;
-        C.d_bres = nullptr;
-        C.cap_jobs = 0;
-        if (cudaMalloc(&C.d_jobs, sizeof(MatrixView) * count) != cudaSuccess ||
-            cudaMalloc(&C.d_bres, sizeof(DevResult) * count) != cudaSuccess)
-            return PBRCM_ERR_OOM;
-        C.cap_jobs = count;
-    }
-    if (!C.d_counter) {
-        if (cudaMalloc(&C.d_counter, sizeof(uint32_t) * 4) != cudaSuccess)
-            return PBRCM_ERR_OOM;
-        C.cap_counter = 4;
-    }
-    // copies in
+    const size_t team_off = align128(off);
+    off = team_off + teamws;
+    if (!grow_dev(C.d_arena, C.cap_arena, off) || !grow_dev(C.d_jobs, C.cap_jobs, count) ||
+        !grow_dev(C.d_bres, C.cap_bres, count) || !grow_dev(C.d_slots, C.cap_slots, nslots) ||
+        !grow_dev(C.d_counter, C.cap_counter, 4))
+        return PBRCM_ERR_OOM;
     unsigned char* A = C.d_arena;
     if (host) {
         for (uint32_t j = 0; j < count; ++j) {
@@ -108,56 +140,49 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
                 return PBRCM_ERR_CUDA;
         }
     }
-    // job table, biggest first; the cutoff sends very large matrices to teams
-    const uint64_t cutoff = (uint64_t)env_int("PBRCM_BATCH_TEAM_CUTOFF_N", 1 << 20);
-    std::vector<uint32_t> order(count);
-    std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(),
-                     [&](uint32_t a, uint32_t b) { return mats[a].nnz > mats[b].nnz; });
-    std::vector<MatrixView> jobs(count);
+    std::vector<BatchJob> jobs(count);
+    std::vector<BatchSlot> slots;
+    slots.reserve(nslots);
+    size_t tw = team_off;
     for (uint32_t q = 0; q < count; ++q) {
         const uint32_t j = order[q];
         const pbrcm_matrix& m = mats[j];
-        MatrixView M{};
-        M.rp = host ? reinterpret_cast<const uint32_t*>(A + slot[j].rp) : m.row_ptr;
-        M.ci = host ? reinterpret_cast<const uint32_t*>(A + slot[j].ci) : m.col_idx;
-        M.n = m.n;
-        M.nnz = (uint32_t)m.nnz;
-        M.claim = reinterpret_cast<uint32_t*>(A + slot[j].claim);
-        M.rec = reinterpret_cast<PosRec*>(A + slot[j].rec);
-        M.perm = host ? reinterpret_cast<uint32_t*>(A + slot[j].perm) : m.perm_out;
-        M.hub = nullptr;
-        M.res = C.d_bres + q;
-        jobs[q] = M;
+        BatchJob& J = jobs[q];
+        std::memset(&J, 0, sizeof(J));
+        J.M.rp = host ? reinterpret_cast<const uint32_t*>(A + slot[j].rp) : m.row_ptr;
+        J.M.ci = host ? reinterpret_cast<const uint32_t*>(A + slot[j].ci) : m.col_idx;
+        J.M.n = m.n;
+        J.M.nnz = (uint32_t)m.nnz;
+        J.M.node = reinterpret_cast<NodeEntry*>(A + slot[j].node);
+        J.M.rec = reinterpret_cast<PosRec*>(A + slot[j].rec);
+        J.M.perm = host ? reinterpret_cast<uint32_t*>(A + slot[j].perm) : m.perm_out;
+        J.M.hub = nullptr;
+        J.M.res = C.d_bres + q;
+        J.team = team[q];
+        if (team[q] > 1) {
+            J.gs = reinterpret_cast<GridSync*>(A + tw);
+            tw = align128(tw + sizeof(GridSync));
+            J.words = reinterpret_cast<unsigned long long*>(A + tw);
+            tw = align128(tw + team_words_bytes((int)team[q]));
+        }
+        for (uint32_t r = 0; r < team[q]; ++r)
+            slots.push_back(BatchSlot{q, r});
     }
-    uint32_t nteam = 0;
-    while (nteam < count && mats[order[nteam]].n > cutoff)
-        ++nteam;
-    if (cudaMemcpyAsync(C.d_jobs, jobs.data(), sizeof(MatrixView) * count, cudaMemcpyHostToDevice, st) !=
+    if (cudaMemcpyAsync(C.d_jobs, jobs.data(), sizeof(BatchJob) * count, cudaMemcpyHostToDevice, st) !=
             cudaSuccess ||
+        cudaMemcpyAsync(C.d_slots, slots.data(), sizeof(BatchSlot) * nslots, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        (teamws && cudaMemsetAsync(A + team_off, 0, teamws, st) != cudaSuccess) ||
         cudaMemsetAsync(C.d_bres, 0, sizeof(DevResult) * count, st) != cudaSuccess ||
         cudaMemsetAsync(C.d_counter, 0, sizeof(uint32_t), st) != cudaSuccess)
         return PBRCM_ERR_CUDA;
     if (launch_validate_batch(C.d_jobs, count, C.sms, st) != cudaSuccess)
         return PBRCM_ERR_CUDA;
     cudaEventRecord(C.ev0, st);
-    // big ones: one team launch each
-    for (uint32_t q = 0; q < nteam; ++q) {
-        if (cudaMemsetAsync(C.d_gs, 0, sizeof(GridSync), st) != cudaSuccess ||
-            launch_team(C.team_variant, jobs[q], opt, C.d_gs, C.d_agg, C.team_ctas, st) != cudaSuccess)
-            return PBRCM_ERR_CUDA;
-    }
-    if (nteam < count) {
-        // the counter starts at nteam: those jobs are done already
-        uint32_t start = nteam;
-        if (cudaMemcpyAsync(C.d_counter, &start, sizeof(uint32_t), cudaMemcpyHostToDevice, st) != cudaSuccess)
-            return PBRCM_ERR_CUDA;
-        int ctas = std::min<int>(batch_max_ctas(C.batch_variant, C.sms), (int)(count - nteam));
-        if (ctas < 1)
-            ctas = 1;
-        if (launch_batch(C.batch_variant, C.d_jobs, count, C.d_counter, opt, ctas, st) != cudaSuccess)
-            return PBRCM_ERR_CUDA;
-    }
+    const int ctas = std::max(1, std::min<int>(maxc, (int)nslots));
+    if (launch_batch(v, C.d_jobs, C.d_slots, (uint32_t)nslots, C.d_counter, opt, ctas, nslots > count, st) !=
+        cudaSuccess)
+        return PBRCM_ERR_CUDA;
     cudaEventRecord(C.ev1, st);
     std::vector<DevResult> res(count);
     if (cudaMemcpyAsync(res.data(), C.d_bres, sizeof(DevResult) * count, cudaMemcpyDeviceToHost, st) !=
@@ -167,18 +192,21 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
     float dms = 0.f;
     cudaEventElapsedTime(&dms, C.ev0, C.ev1);
     // matrices with a hub row rerun on the team path with hub scratch
+    Options topt = make_options(opts, kModeFull);
+    apply_team_shape(C, topt);
     for (uint32_t q = 0; q < count; ++q) {
         if (res[q].status != kNeedHub)
             continue;
-        const MatrixView& M = jobs[q];
+        const MatrixView& M = jobs[q].M;
         if (!C.ensure_hub(M.nnz))
             return PBRCM_ERR_OOM;
         MatrixView H = M;
         H.hub = C.d_hub;
         if (cudaMemsetAsync(M.res, 0, sizeof(DevResult), st) != cudaSuccess ||
             cudaMemsetAsync(C.d_gs, 0, sizeof(GridSync), st) != cudaSuccess ||
+            cudaMemsetAsync(C.d_agg, 0, team_words_bytes(C.team_ctas), st) != cudaSuccess ||
             launch_validate(M.rp, M.ci, M.n, M.nnz, M.res, C.sms, st) != cudaSuccess ||
-            launch_team(C.team_variant, H, opt, C.d_gs, C.d_agg, C.team_ctas, st) != cudaSuccess ||
+            launch_team(C.team_variant, H, topt, C.d_gs, C.d_agg, C.team_ctas, st) != cudaSuccess ||
             cudaMemcpyAsync(&res[q], M.res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess)
             return PBRCM_ERR_CUDA;
@@ -187,7 +215,7 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
     for (uint32_t q = 0; q < count; ++q) {
         const uint32_t j = order[q];
         if (host && res[q].status == kOk) {
-            if (cudaMemcpyAsync(mats[j].perm_out, jobs[q].perm, 4 * (size_t)mats[j].n, cudaMemcpyDeviceToHost,
+            if (cudaMemcpyAsync(mats[j].perm_out, jobs[q].M.perm, 4 * (size_t)mats[j].n, cudaMemcpyDeviceToHost,
                                 st) != cudaSuccess)
                 return PBRCM_ERR_CUDA;
         }
@@ -201,7 +229,7 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
     if (cudaStreamSynchronize(st) != cudaSuccess)
         return PBRCM_ERR_CUDA;
     if (results) {
-        float tms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        const float tms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
         for (uint32_t j = 0; j < count; ++j)
             results[j].total_ms = tms;
     }
@@ -209,14 +237,6 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
 }
 
 }  // namespace
-
-#define PBRCM_CTX2(ctx)                                      \
-    if (!ctx) {                                              \
-        int32_t rc_ = pbrcm_context_create(-1, &ctx_local); \
-        if (rc_ != PBRCM_OK)                                 \
-            return rc_;                                      \
-        ctx = ctx_local;                                     \
-    }
 
 extern "C" {
 
@@ -228,7 +248,12 @@ int32_t pbrcm_reorder_batch(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32
     if (count == 0)
         return PBRCM_OK;
     pbrcm_context* ctx_local = nullptr;
-    PBRCM_CTX2(ctx);
+    if (!ctx) {
+        int32_t rc = pbrcm_context_create(-1, &ctx_local);
+        if (rc != PBRCM_OK)
+            return rc;
+        ctx = ctx_local;
+    }
     int32_t rc;
     {
         std::lock_guard<std::mutex> lk(ctx->ctx.mu);
@@ -248,13 +273,18 @@ int32_t pbrcm_reorder_batch_device(pbrcm_context* ctx, const pbrcm_matrix* mats,
     if (count == 0)
         return PBRCM_OK;
     pbrcm_context* ctx_local = nullptr;
-    PBRCM_CTX2(ctx);
+    if (!ctx) {
+        int32_t rc = pbrcm_context_create(-1, &ctx_local);
+        if (rc != PBRCM_OK)
+            return rc;
+        ctx = ctx_local;
+    }
     int32_t rc;
     {
         std::lock_guard<std::mutex> lk(ctx->ctx.mu);
         cudaSetDevice(ctx->ctx.device);
-        rc = run_batch(ctx->ctx, mats, count, opts, results,
-                       stream ? (cudaStream_t)stream : ctx->ctx.stream, false);
+        rc = run_batch(ctx->ctx, mats, count, opts, results, stream ? (cudaStream_t)stream : ctx->ctx.stream,
+                       false);
     }
     if (ctx_local)
         pbrcm_context_destroy(ctx_local);

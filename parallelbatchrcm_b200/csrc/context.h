@@ -17,17 +17,21 @@ struct Context {
     int sms = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    int team_variant = 2;   // kernel shape of the one-matrix team
+    int team_variant = 1;   // kernel shape of the one-matrix team
     int team_ctas = 0;      // CTAs of the one-matrix team
-    int batch_variant = 1;  // kernel shape of the one-CTA-per-matrix batch
+    int batch_variant = 2;  // kernel shape of the batch kernel
+    uint32_t solo_edges = 0;    // levels at most this big run on one CTA
+    uint32_t solo_parents = 0;
+    uint32_t barrier = 0;       // team barrier implementation
+    int team_maxc = 0;          // co-resident CTAs of the team kernel
 
     // single-matrix buffers (grow only)
     uint32_t* d_rp = nullptr;
     size_t cap_rp = 0;
     uint32_t* d_ci = nullptr;
     size_t cap_ci = 0;
-    uint32_t* d_claim = nullptr;
-    size_t cap_claim = 0;
+    NodeEntry* d_node = nullptr;
+    size_t cap_node = 0;
     uint32_t* d_perm = nullptr;
     size_t cap_perm = 0;
     PosRec* d_rec = nullptr;
@@ -40,19 +44,16 @@ struct Context {
     unsigned long long* d_agg = nullptr;
 
     // batch buffers (grow only)
-    MatrixView* d_jobs = nullptr;
+    BatchJob* d_jobs = nullptr;
     size_t cap_jobs = 0;
+    BatchSlot* d_slots = nullptr;
+    size_t cap_slots = 0;
     uint32_t* d_counter = nullptr;
     size_t cap_counter = 0;
     DevResult* d_bres = nullptr;
     size_t cap_bres = 0;
     unsigned char* d_arena = nullptr;
     size_t cap_arena = 0;
-
-    // per-stream aggregate arrays of the serving session's team launches
-    unsigned long long* d_agg_session = nullptr;
-    size_t cap_agg_session = 0;
-    unsigned long long* d_agg_session_slot(int stream_index);
 
     int32_t init(int dev);
     ~Context();
@@ -64,6 +65,7 @@ struct Context {
 
 int32_t map_status(uint32_t s);
 Options make_options(const struct pbrcm_options* o, uint32_t mode);
+void apply_team_shape(const Context& C, Options& opt);
 void fill_result(const DevResult& r, const Options& opt, struct pbrcm_result* out);
 
 }  // namespace pbrcm

@@ -2,40 +2,46 @@
 //
 // What it computes
 //   The serial stable Cuthill-McKee order of the reference
-//   (src/rcm_cpu.cpp:57-104): FIFO over positions; parent at position i
+//   (src/rcm_cpu.cpp:57-104): FIFO over positions; the parent at position i
 //   appends its still-unvisited neighbours, stable-sorted by valence (row
-//   length).  The reference's GPU_BATCH reaches it with a chain of speculative
-//   batches (include/device/batchWorker.cuh); this engine reaches it level by
-//   level with every CTA of a team working on one BFS level at a time.
+//   length).  The reference's GPU_BATCH reaches it with a chain of
+//   speculative batches (include/device/batchWorker.cuh); this engine reaches
+//   it level by level, every CTA of a team working on one BFS level at a time.
 //
 // The claim key
-//   Edges of the frontier are numbered in queue order: edge (position i, slot
-//   k) has the global id ebase(i) + k, where ebase(i) = sum of the valences of
-//   the nodes at positions < i.  Every frontier edge does
-//   atomicMin(claim[child], id + 1).  Once a level's claims are done, a node's
-//   claim is the id + 1 of the FIRST edge that reaches it in queue order --
-//   exactly the (parent, slot) that discovers it in the serial algorithm,
-//   duplicates in a row included.  An edge is a "child edge" iff
-//   claim[col] == id + 1, a purely local test.  The key is an order-preserving
-//   lexicographic (parent position, slot) code; the reference's batch code
+//   Within one BFS pass the edges are numbered in queue order: edge (position
+//   i, slot k) has id ebase(i) + k, where ebase(i) = sum of the valences at
+//   positions < i.  Pass p owns the key range [p*kspan, p*kspan + nnz + 1]
+//   (kspan = nnz + 2); edge id e maps to key base_p - 1 - e with
+//   base_p = p*kspan + nnz + 1 (the start node takes base_p itself).  Every
+//   frontier edge does atomicMax(node[child].claim, key).  Once a level's
+//   claims are done, a node's claim is the key of the FIRST edge that reaches
+//   it in queue order -- exactly the (parent, slot) that discovers it in the
+//   serial algorithm, duplicate entries included -- so an edge is a child
+//   edge iff node[col].claim == its key: a purely local test.  Keys of later
+//   levels are smaller, so claiming for the next level never disturbs a node
+//   already placed, and keys of a later pass are larger than every key of an
+//   earlier one, so passes need no reset.  The key is an order-preserving
+//   (parent position, slot) code; the reference's batch code
 //   (batchId << 11 | offset, batchWorker.cuh:574-586) plays the same role for
 //   its batches.
 //
-// One level (frontier = positions [a, b), its edges have ids [Ka, Kb))
+// One level (frontier = positions [a, b), edge ids [Ka, Kb))
 //   collect: each CTA takes a contiguous range of parents, splits it into
-//            chunks (<= B parents, <= EMAX edges), finds the child edges,
-//            compacts them in (parent, slot) order and sorts each parent's
-//            children by (valence, slot) with a counting rank.
+//            chunks (<= B parents, <= EMAX edges), reads one node entry per
+//            edge (claim + row start + valence in one 16-byte load), keeps
+//            the child edges in (parent, slot) order and ranks every
+//            parent's children by (valence, slot).
 //   place:   children get positions b + (children of earlier parents) + rank
-//            and edge bases Kb + (valences of earlier children); their
-//            records go to rec[], the output to perm[].
-//   claim:   the placed children immediately claim their own edges for the
-//            next level.  Keys of the next level are > Kb, so they never
-//            disturb nodes already placed (their claims are <= Kb).
-//   A team of one CTA places chunk by chunk with a running offset; a grid
-//   team publishes per-CTA totals, meets at a barrier, then places.
-//   Parents with more than EMAX edges ("hubs") are collected and
-//   radix-sorted in global scratch by one CTA.
+//            and edge bases Kb + (valences of earlier children): records to
+//            rec[], the node to perm[].
+//   claim:   the placed children claim their own edges for the next level.
+//   A grid team publishes per-CTA (children, valence) totals with a
+//   level-tagged all-gather, places, and meets at a barrier.  Levels with a
+//   small frontier run on CTA 0 alone ("solo") with block barriers only; the
+//   other CTAs park at a gate until CTA 0 hands a large level back.  Parents
+//   with more than EMAX edges ("hubs") are collected and radix-sorted in
+//   global scratch by one CTA.
 //
 // Every wait is bounded by %globaltimer and reports PBRCM_ERR_TIMEOUT.
 // With PBRCM_CHECKS defined, every global index is range-checked and a
@@ -66,14 +72,31 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p)
     return v;
 }
 
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 __device__ __forceinline__ void st_release(unsigned int* p, unsigned int v)
 {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
+__device__ __forceinline__ void red_release_add(unsigned int* p, unsigned int v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 __device__ __forceinline__ uint32_t ld_ro(const uint32_t* p) { return __ldg(p); }
+
+__device__ __forceinline__ uint4 ld_node(const NodeEntry* p) { return __ldcg(reinterpret_cast<const uint4*>(p)); }
 
 __device__ __forceinline__ void set_status(DevResult* r, uint32_t code, uint32_t where)
 {
@@ -128,6 +151,35 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T& total, T* tmp)
     return r;
 }
 
+// Block-wide exclusive scan with a single barrier.  `buf` (B/32 entries) must
+// belong to this call site alone: it is read after the barrier and not
+// cleared, so the next write to it must come after another block barrier.
+template <int B>
+__device__ __forceinline__ uint32_t block_scan1(uint32_t v, uint32_t& total, uint32_t* buf)
+{
+    constexpr int W = B / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o)
+            x += y;
+    }
+    if (lane == 31)
+        buf[w] = x;
+    __syncthreads();
+    uint32_t before = 0, all = 0;
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+        const uint32_t b = buf[i];
+        before += i < w ? b : 0u;
+        all += b;
+    }
+    total = all;
+    return before + x - v;
+}
+
 template <int B, typename T>
 __device__ __forceinline__ T block_reduce_max(T v, T* tmp)
 {
@@ -166,63 +218,128 @@ __device__ __forceinline__ T block_reduce_sum(T v, T* tmp)
     return r;
 }
 
+// Two sums at once (tmp holds 2 * (B/32) entries).
+template <int B>
+__device__ __forceinline__ void block_reduce_sum2(unsigned long long& a, unsigned long long& b,
+                                                  unsigned long long* tmp)
+{
+    constexpr int W = B / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(kFull, a, o);
+        b += __shfl_xor_sync(kFull, b, o);
+    }
+    if (lane == 0) {
+        tmp[w] = a;
+        tmp[W + w] = b;
+    }
+    __syncthreads();
+    unsigned long long ra = 0, rb = 0;
+    for (int i = 0; i < W; ++i) {
+        ra += tmp[i];
+        rb += tmp[W + i];
+    }
+    a = ra;
+    b = rb;
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
-// Team: one CTA, or all CTAs of a cooperative launch (grid barrier).
+// Team: one CTA, or all CTAs of a cooperative launch.
 // ---------------------------------------------------------------------------
 struct Team {
     GridSync* gs;        // nullptr for a one-CTA team
+    unsigned int* flags; // one barrier flag word per CTA (+ phantom), zeroed per launch
     uint32_t size;       // CTAs in the team
     uint32_t rank;       // this CTA
-    uint32_t expected;   // arrivals a barrier waits for (size + phantom)
-    unsigned int gen;    // local barrier generation
+    uint32_t expected;   // CTAs a barrier waits for (size + phantom)
+    uint32_t target;     // barriers passed so far
+    uint32_t mode;       // barrier implementation (see sync)
+    uint32_t epoch;      // gate epochs seen
     unsigned long long wait_ns;
     DevResult* res;
 
-    // Returns false if the team must stop (error anywhere or timeout).
+    // Block-uniform "keep going?" after a block barrier.
+    __device__ bool block_ok()
+    {
+        __shared__ int s_ok;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_ok = read_status(res) == 0;
+        __syncthreads();
+        return s_ok != 0;
+    }
+
+    // Team barrier, two implementations (Options::barrier):
+    //  0  monotonic counter: one release-add per CTA on gs->count, thread 0
+    //     acquire-polls until it reaches (barriers so far) x (team size);
+    //  1  flag array: every CTA release-stores the barrier's sequence number
+    //     into its own flag word; threads i < expected poll flag i with
+    //     relaxed loads, then fence (acquire pattern).
+    // Returns false if the team must stop (an error anywhere, or the wait
+    // ran out).
     __device__ bool sync(uint32_t where)
     {
         __shared__ int s_ok;
-        if (gs == nullptr) {
-            // one CTA: thread 0 reads the status once so that every thread
-            // takes the same branch afterwards
-            __syncthreads();
-            if (threadIdx.x == 0)
-                s_ok = read_status(res) == 0;
-            __syncthreads();
-            return s_ok != 0;
-        }
+        if (gs == nullptr)
+            return block_ok();
+        target += 1;
+        if (threadIdx.x == 0)
+            s_ok = 1;
         __syncthreads();
-        if (threadIdx.x == 0) {
-            int ok = 1;
-            __threadfence();
-            unsigned int prev = atomicAdd(&gs->arrive, 1u);
-            if (prev == expected - 1) {
-                atomicExch(&gs->arrive, 0u);
-                __threadfence();
-                st_release(&gs->gen, gen + 1);
-            } else {
-                unsigned long long t0 = globaltimer();
-                unsigned int spins = 0;
-                while (ld_acquire(&gs->gen) == gen) {
-                    if (read_status(res) != 0) {
-                        ok = 0;
+        if (mode == 0) {
+            if (threadIdx.x == 0) {
+                red_release_add(&gs->count, 1u);
+                const uint32_t goal = target * expected;
+                unsigned long long t0 = 0;
+                uint32_t spins = 0;
+                while ((int)(ld_acquire(&gs->count) - goal) < 0) {
+                    if ((++spins & 31u) == 0 && !wait_check(t0, where)) {
+                        s_ok = 0;
                         break;
                     }
-                    if ((++spins & 63u) == 0 && globaltimer() - t0 > wait_ns) {
-                        set_status(res, kErrTimeout, where);
-                        ok = 0;
+                    if (spins > 2048)
+                        __nanosleep(128);
+                }
+            }
+        } else {
+            if (threadIdx.x == 0)
+                st_release(flags + rank, target);
+            for (uint32_t i = threadIdx.x; i < expected; i += blockDim.x) {
+                unsigned long long t0 = 0;
+                uint32_t spins = 0;
+                while ((int)(*reinterpret_cast<volatile unsigned int*>(flags + i) - target) < 0) {
+                    if ((++spins & 31u) == 0 && !wait_check(t0, where)) {
+                        s_ok = 0;
                         break;
                     }
                     if (spins > 256)
                         __nanosleep(64);
                 }
+                __threadfence();
             }
-            gen += 1;
-            __threadfence();
-            s_ok = ok && read_status(res) == 0;
         }
         __syncthreads();
-        return s_ok != 0;
+        const int ok = s_ok && read_status(res) == 0;
+        __syncthreads();
+        return ok != 0;
+    }
+
+    // Shared by every bounded wait: false once an error is posted or the
+    // wait has run longer than wait_ns (then it posts PBRCM_ERR_TIMEOUT).
+    __device__ __forceinline__ bool wait_check(unsigned long long& t0, uint32_t where)
+    {
+        if (read_status(res) != 0)
+            return false;
+        const unsigned long long now = globaltimer();
+        if (t0 == 0) {
+            t0 = now;
+        } else if (now - t0 > wait_ns) {
+            set_status(res, kErrTimeout, where);
+            return false;
+        }
+        return true;
     }
 };
 
@@ -232,6 +349,7 @@ struct Team {
 template <int B, int EMAX>
 struct Smem {
     static constexpr int W = B / 32;
+    static constexpr int PREMAX = 4 * EMAX;  // prefetched child adjacency
     // parents of the current chunk
     uint32_t pn[B], prs[B], pdeg[B], peb[B];
     uint32_t soff[B + 1];   // edge offset of parent j inside the chunk
@@ -245,13 +363,16 @@ struct Smem {
         };
         uint32_t hcnt[W * 256];
     };
-    uint32_t so_idx[EMAX];       // sorted position -> compacted index
-    uint32_t so_eoff[EMAX + 1];  // edge offset of the child at sorted position
+    uint32_t so_idx[EMAX];       // ranked position -> compacted index
+    uint32_t so_eoff[EMAX + 1];  // edge offset of the child at ranked position
+    uint32_t pre[PREMAX];        // children's adjacency loaded ahead of the all-gather
     uint32_t tmp32[W + 1];
-    unsigned long long tmp64[W + 1];
+    unsigned long long tmp64[2 * W + 2];
+    unsigned long long gat64[2 * W + 2];  // all-gather reduction (its own buffer)
+    uint32_t scanbuf[5][W];               // one per block_scan1 call site
     uint32_t hist[256];
     // chunk scalars
-    uint32_t m, Ec, Q, Qdeg, hub;
+    uint32_t m, Ec, Q, Qdeg, hub, npre;
     uint32_t bcast[8];
 };
 
@@ -270,6 +391,7 @@ struct Chunk {
     static_assert(EMAX % B == 0, "EMAX must be a multiple of B");
     Smem<B, EMAX>& s;
     const MatrixView& M;
+    uint32_t base;  // key of the pass: edge id e has key base - 1 - e
 
     // Loads up to B parents starting at position p (< pend) and forms the
     // next chunk: the longest run with <= EMAX edges.  Sets s.m (0 = the
@@ -281,9 +403,9 @@ struct Chunk {
         uint32_t deg = 0;
         const bool have = p + t < pend;
         if (have) {
-            uint32_t pos = p + t;
+            const uint32_t pos = p + t;
             if (PB_CHECK(M.res, pos < M.n, 101)) {
-                uint4 r = __ldcg(reinterpret_cast<const uint4*>(M.rec) + pos);
+                const uint4 r = __ldcg(reinterpret_cast<const uint4*>(M.rec) + pos);
                 s.pn[t] = r.x;
                 s.prs[t] = r.y;
                 s.pdeg[t] = r.z;
@@ -291,24 +413,23 @@ struct Chunk {
                 deg = r.z;
             }
         }
+        s.cc[t] = 0;
         uint32_t total;
-        uint32_t excl = block_exclusive_scan<B, uint32_t>(deg, total, s.tmp32);
-        // parents whose inclusive edge count stays within EMAX
-        uint32_t incl = excl + deg;
-        int fits = have && incl <= (uint32_t)EMAX && excl <= (uint32_t)EMAX;
-        int m = __syncthreads_count(fits);
+        const uint32_t excl = block_scan1<B>(deg, total, s.scanbuf[0]);
+        const uint32_t incl = excl + deg;
         // incl is monotone in t, so the fitting parents are a prefix
+        const int fits = have && incl <= (uint32_t)EMAX;
+        const int m = __syncthreads_count(fits);
         if (fits)
             s.soff[t] = excl;
+        if (m > 0 && t == (uint32_t)(m - 1))
+            s.soff[m] = incl;
         if (t == 0) {
             s.m = (uint32_t)m;
             s.hub = (m == 0 && p < pend) ? 1u : 0u;
+            if (m == 0)
+                s.soff[0] = 0;
         }
-        __syncthreads();
-        if (t == (uint32_t)(m > 0 ? m - 1 : 0) && m > 0)
-            s.soff[m] = incl;
-        if (t == 0 && m == 0)
-            s.soff[0] = 0;
         __syncthreads();
         if (t == 0)
             s.Ec = m > 0 ? s.soff[m] : 0;
@@ -316,24 +437,21 @@ struct Chunk {
         return m > 0 ? (uint32_t)m : (p < pend ? 1u : 0u);
     }
 
-    // Finds the child edges of the chunk, compacts them, sorts every parent's
-    // children (sorted = by valence, stable; else slot order) and computes the
-    // edge offsets of the sorted children.  Returns (children, valence sum).
+    // Finds the child edges of the chunk, compacts them, ranks every
+    // parent's children (sorted = by valence, stable; else slot order) and
+    // computes the edge offsets of the ranked children.
     __device__ Agg collect(bool sorted)
     {
         const uint32_t t = threadIdx.x;
         const uint32_t m = s.m, Ec = s.Ec;
-        if (t < m)
-            s.cc[t] = 0;
         const uint32_t ept = (Ec + B - 1) / B;
         const uint32_t e0 = t * ept;
         const uint32_t e1 = min(e0 + ept, Ec);
-        // parent of e0: largest j with soff[j] <= e0
         uint32_t j = 0;
         if (e0 < e1) {
             uint32_t lo = 0, hi = m;  // soff[lo] <= e0 < soff[hi]
             while (hi - lo > 1) {
-                uint32_t mid = (lo + hi) >> 1;
+                const uint32_t mid = (lo + hi) >> 1;
                 if (s.soff[mid] <= e0)
                     lo = mid;
                 else
@@ -341,7 +459,6 @@ struct Chunk {
             }
             j = lo;
         }
-        __syncthreads();  // cc zeroed
         uint32_t c[MAXEPT], jj[MAXEPT], key[MAXEPT], kk[MAXEPT];
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
@@ -350,37 +467,32 @@ struct Chunk {
             if (e < e1) {
                 while (s.soff[j + 1] <= e)
                     ++j;
-                uint32_t k = e - s.soff[j];
-                uint32_t idx = s.prs[j] + k;
+                const uint32_t k = e - s.soff[j];
+                const uint32_t idx = s.prs[j] + k;
                 jj[r] = j;
                 kk[r] = k;
-                key[r] = s.peb[j] + k + 1;
+                key[r] = base - 1u - (s.peb[j] + k);
                 if (PB_CHECK(M.res, idx < M.nnz, 102))
                     c[r] = ld_ro(M.ci + idx);
             }
         }
-        uint32_t cl[MAXEPT];
+        uint4 nd[MAXEPT];
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
-            cl[r] = 0;
+            nd[r] = make_uint4(0, 0, 0, 0);
             if (c[r] != kUnvisited && PB_CHECK(M.res, c[r] < M.n, 103))
-                cl[r] = ld_cg(M.claim + c[r]);
+                nd[r] = ld_node(M.node + c[r]);
         }
-        uint32_t r0[MAXEPT], r1[MAXEPT];
         uint32_t nvalid = 0;
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
-            const bool valid = c[r] != kUnvisited && c[r] < M.n && cl[r] == key[r];
-            if (valid) {
-                r0[r] = ld_ro(M.rp + c[r]);
-                r1[r] = ld_ro(M.rp + c[r] + 1);
+            if (c[r] != kUnvisited && c[r] < M.n && nd[r].x == key[r])
                 ++nvalid;
-            } else {
+            else
                 c[r] = kUnvisited;
-            }
         }
         uint32_t Q;
-        uint32_t q = block_exclusive_scan<B, uint32_t>(nvalid, Q, s.tmp32);
+        uint32_t q = block_scan1<B>(nvalid, Q, s.scanbuf[1]);
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
             const uint32_t e = e0 + r;
@@ -390,8 +502,8 @@ struct Chunk {
                 if (c[r] != kUnvisited) {
                     if (PB_CHECK(M.res, q < (uint32_t)EMAX, 104)) {
                         s.ch_node[q] = c[r];
-                        s.ch_rs[q] = r0[r];
-                        s.ch_deg[q] = r1[r] - r0[r];
+                        s.ch_rs[q] = nd[r].y;
+                        s.ch_deg[q] = nd[r].z;
                         s.ch_par[q] = jj[r];
                         atomicAdd(&s.cc[jj[r]], 1u);
                     }
@@ -416,14 +528,14 @@ struct Chunk {
             s.so_idx[st + rank] = x;
         }
         __syncthreads();
-        // edge offsets in sorted order (blocked exclusive scan)
+        // edge offsets in ranked order (blocked exclusive scan)
         const uint32_t per = (Q + B - 1) / B;
         const uint32_t i0 = min(t * per, Q), i1 = min(i0 + per, Q);
         uint32_t loc = 0;
         for (uint32_t i = i0; i < i1; ++i)
             loc += s.ch_deg[s.so_idx[i]];
         uint32_t Qdeg;
-        uint32_t off = block_exclusive_scan<B, uint32_t>(loc, Qdeg, s.tmp32);
+        uint32_t off = block_scan1<B>(loc, Qdeg, s.scanbuf[2]);
         for (uint32_t i = i0; i < i1; ++i) {
             s.so_eoff[i] = off;
             off += s.ch_deg[s.so_idx[i]];
@@ -432,44 +544,99 @@ struct Chunk {
             s.so_eoff[Q] = Qdeg;
             s.Q = Q;
             s.Qdeg = Qdeg;
+            s.npre = 0;
         }
         __syncthreads();
         return Agg{Q, Qdeg};
     }
 
-    // Writes the sorted children of the chunk at positions P0.. and edge
+    // The ranked child owning edge offset f: so_eoff[lo] <= f < so_eoff[lo+1].
+    __device__ __forceinline__ uint32_t child_of(uint32_t f) const
+    {
+        uint32_t lo = 0, hi = s.Q;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s.so_eoff[mid] <= f)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        return lo;
+    }
+
+    // Walks the ranked children's edges in blocks of consecutive edge offsets
+    // (one search per thread, then a forward walk), calling
+    // fn(f, col_index) for each.
+    template <typename Fn>
+    __device__ __forceinline__ void for_child_edges(Fn fn) const
+    {
+        const uint32_t Qdeg = s.Qdeg;
+        const uint32_t per = (Qdeg + B - 1) / B;
+        const uint32_t f0 = threadIdx.x * per, f1 = min(f0 + per, Qdeg);
+        if (f0 >= f1)
+            return;
+        uint32_t lo = child_of(f0);
+        uint32_t beg = s.so_eoff[lo], nxt = s.so_eoff[lo + 1];
+        uint32_t rs = s.ch_rs[s.so_idx[lo]];
+        for (uint32_t f = f0; f < f1; ++f) {
+            while (f >= nxt) {
+                ++lo;
+                beg = nxt;
+                nxt = s.so_eoff[lo + 1];
+                rs = s.ch_rs[s.so_idx[lo]];
+            }
+            fn(f, rs + (f - beg));
+        }
+    }
+
+    // Loads the ranked children's adjacency into s.pre (when it fits) so that
+    // the claims after the all-gather issue no dependent load.
+    __device__ void prefetch()
+    {
+        const uint32_t Qdeg = s.Qdeg;
+        if (Qdeg > (uint32_t)Smem<B, EMAX>::PREMAX)
+            return;
+        for_child_edges([&](uint32_t f, uint32_t idx) {
+            s.pre[f] = PB_CHECK(M.res, idx < M.nnz, 108) ? ld_ro(M.ci + idx) : 0u;
+        });
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s.npre = Qdeg;
+        __syncthreads();
+    }
+
+    // Writes the ranked children of the chunk at positions P0.. and edge
     // bases K0.., then claims their edges for the next level.
     __device__ void place_and_claim(uint32_t P0, uint32_t K0, bool write_perm, bool reverse)
     {
         const uint32_t t = threadIdx.x;
         const uint32_t Q = s.Q, Qdeg = s.Qdeg;
+        const bool have_pre = s.npre == Qdeg && Qdeg > 0;
         for (uint32_t i = t; i < Q; i += B) {
             const uint32_t x = s.so_idx[i];
             const uint32_t pos = P0 + i;
             if (PB_CHECK(M.res, pos < M.n, 105)) {
-                uint4 r = make_uint4(s.ch_node[x], s.ch_rs[x], s.ch_deg[x], K0 + s.so_eoff[i]);
+                const uint4 r = make_uint4(s.ch_node[x], s.ch_rs[x], s.ch_deg[x], K0 + s.so_eoff[i]);
                 __stcg(reinterpret_cast<uint4*>(M.rec) + pos, r);
                 if (write_perm)
                     M.perm[reverse ? M.n - 1 - pos : pos] = r.x;
             }
         }
-        // claims: edge-parallel over the children's rows
-        for (uint32_t f = t; f < Qdeg; f += B) {
-            uint32_t lo = 0, hi = Q;  // so_eoff[lo] <= f < so_eoff[hi]
-            while (hi - lo > 1) {
-                uint32_t mid = (lo + hi) >> 1;
-                if (s.so_eoff[mid] <= f)
-                    lo = mid;
-                else
-                    hi = mid;
-            }
-            const uint32_t x = s.so_idx[lo];
-            const uint32_t idx = s.ch_rs[x] + (f - s.so_eoff[lo]);
-            if (PB_CHECK(M.res, idx < M.nnz, 106)) {
-                const uint32_t d = ld_ro(M.ci + idx);
+        const uint32_t kb = base - 1u - K0;
+        if (have_pre) {
+            for (uint32_t f = t; f < Qdeg; f += B) {
+                const uint32_t d = s.pre[f];
                 if (PB_CHECK(M.res, d < M.n, 107))
-                    atomicMin(M.claim + d, K0 + f + 1);
+                    atomicMax(&M.node[d].claim, kb - f);
             }
+        } else {
+            for_child_edges([&](uint32_t f, uint32_t idx) {
+                if (PB_CHECK(M.res, idx < M.nnz, 106)) {
+                    const uint32_t d = ld_ro(M.ci + idx);
+                    if (PB_CHECK(M.res, d < M.n, 107))
+                        atomicMax(&M.node[d].claim, kb - f);
+                }
+            });
         }
     }
 
@@ -496,25 +663,28 @@ struct Chunk {
         unsigned long long Qdeg = 0;
         uint32_t maxkey = 0;
         constexpr uint32_t TILE = B * MAXEPT;
-        for (uint32_t base = 0; base < D; base += TILE) {
+        for (uint32_t base0 = 0; base0 < D; base0 += TILE) {
             uint32_t nv = 0;
             uint32_t dg[MAXEPT];
             bool ok[MAXEPT];
 #pragma unroll
             for (int r = 0; r < MAXEPT; ++r) {
-                const uint32_t e = base + t * MAXEPT + r;
+                const uint32_t e = base0 + t * MAXEPT + r;
                 ok[r] = false;
                 if (e < D && PB_CHECK(M.res, rs + e < M.nnz, 121)) {
                     const uint32_t c = ld_ro(M.ci + rs + e);
-                    if (PB_CHECK(M.res, c < M.n, 122) && ld_cg(M.claim + c) == eb + e + 1) {
-                        dg[r] = ld_ro(M.rp + c + 1) - ld_ro(M.rp + c);
-                        ok[r] = true;
-                        ++nv;
+                    if (PB_CHECK(M.res, c < M.n, 122)) {
+                        const uint4 nd = ld_node(M.node + c);
+                        if (nd.x == base - 1u - (eb + e)) {
+                            dg[r] = nd.z;
+                            ok[r] = true;
+                            ++nv;
+                        }
                     }
                 }
             }
             uint32_t tot;
-            uint32_t q = block_exclusive_scan<B, uint32_t>(nv, tot, s.tmp32);
+            uint32_t q = block_scan1<B>(nv, tot, s.scanbuf[3]);
             uint32_t lsum = 0, lmax = 0;
 #pragma unroll
             for (int r = 0; r < MAXEPT; ++r) {
@@ -522,7 +692,7 @@ struct Chunk {
                     const uint32_t w = r0 + Q + q;
                     if (PB_CHECK(M.res, w < M.nnz, 123)) {
                         hk0()[w] = dg[r];
-                        hv0()[w] = base + t * MAXEPT + r;
+                        hv0()[w] = base0 + t * MAXEPT + r;
                     }
                     lsum += dg[r];
                     lmax = max(lmax, dg[r]);
@@ -572,17 +742,17 @@ struct Chunk {
         if (t == 0) {
             uint32_t run = 0;
             for (int d = 0; d < 256; ++d) {
-                uint32_t h = s.hist[d];
+                const uint32_t h = s.hist[d];
                 s.hist[d] = run;
                 run += h;
             }
         }
         __syncthreads();
-        for (uint32_t base = 0; base < Q; base += B) {
+        for (uint32_t base0 = 0; base0 < Q; base0 += B) {
             for (uint32_t i = t; i < (uint32_t)(Smem<B, EMAX>::W * 256); i += B)
                 s.hcnt[i] = 0;
             __syncthreads();
-            const uint32_t i = base + t;
+            const uint32_t i = base0 + t;
             const bool act = i < Q;
             uint32_t key = 0, val = 0, dgt = 0;
             if (act) {
@@ -627,21 +797,20 @@ struct Chunk {
         while (done < Q) {
             const uint32_t cnt = min((uint32_t)EMAX, Q - done);
             uint32_t loc = 0;
-            // blocked layout for the scan
             const uint32_t per = (cnt + B - 1) / B;
             const uint32_t i0 = min(t * per, cnt), i1 = min(i0 + per, cnt);
             for (uint32_t i = i0; i < i1; ++i) {
                 const uint32_t slot = __ldcg(hv0() + r0 + done + i);
                 const uint32_t node = ld_ro(M.ci + rs + slot);
-                const uint32_t a = ld_ro(M.rp + node), b = ld_ro(M.rp + node + 1);
+                const uint4 nd = ld_node(M.node + node);
                 s.ch_node[i] = node;
-                s.ch_rs[i] = a;
-                s.ch_deg[i] = b - a;
+                s.ch_rs[i] = nd.y;
+                s.ch_deg[i] = nd.z;
                 s.so_idx[i] = i;
-                loc += b - a;
+                loc += nd.z;
             }
             uint32_t tot;
-            uint32_t off = block_exclusive_scan<B, uint32_t>(loc, tot, s.tmp32);
+            uint32_t off = block_scan1<B>(loc, tot, s.scanbuf[4]);
             for (uint32_t i = i0; i < i1; ++i) {
                 s.so_eoff[i] = off;
                 off += s.ch_deg[i];
@@ -650,6 +819,7 @@ struct Chunk {
                 s.so_eoff[cnt] = tot;
                 s.Q = cnt;
                 s.Qdeg = tot;
+                s.npre = 0;
             }
             __syncthreads();
             place_and_claim(P0 + done, K0 + kdone, write_perm, reverse);
@@ -661,31 +831,113 @@ struct Chunk {
 };
 
 // ---------------------------------------------------------------------------
-// One ordered BFS pass from `start`.  Fills rec[0..placed) and, when
-// write_perm, the output.  Returns false if the team must stop.
-// level_out: number of levels; last_start: first position of the last level.
+// Level state of one pass.
+// ---------------------------------------------------------------------------
+struct LevelState {
+    uint32_t a, b;     // frontier positions [a, b)
+    uint32_t Ka, Kb;   // edge ids of the frontier [Ka, Kb)
+    uint32_t L;        // level index of the frontier
+    uint32_t last_start;
+};
+
+// Bounded wait at the gate for CTA 0 to hand a solo run back.  Thread 0
+// polls; the wait only runs out if CTA 0's heartbeat stops for wait_ns.
+__device__ __forceinline__ bool gate_wait(Team& team, LevelState& st)
+{
+    __shared__ int s_ok;
+    __shared__ uint32_t s_st[6];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const uint32_t want = team.epoch + 1;
+        unsigned long long t0 = globaltimer();
+        uint32_t hb = *reinterpret_cast<volatile uint32_t*>(&team.gs->heartbeat);
+        uint32_t spins = 0;
+        while ((int)(ld_acquire(&team.gs->epoch) - want) < 0) {
+            if ((++spins & 63u) == 0) {
+                if (read_status(team.res) != 0) {
+                    ok = 0;
+                    break;
+                }
+                const uint32_t h = *reinterpret_cast<volatile uint32_t*>(&team.gs->heartbeat);
+                const unsigned long long now = globaltimer();
+                if (h != hb) {
+                    hb = h;
+                    t0 = now;
+                } else if (now - t0 > team.wait_ns) {
+                    set_status(team.res, kErrTimeout, 50);
+                    ok = 0;
+                    break;
+                }
+            }
+            if (spins > 1024)
+                __nanosleep(256);
+        }
+        if (ok)
+            for (int i = 0; i < 6; ++i)
+                s_st[i] = __ldcg(&team.gs->st[i]);
+        s_ok = ok && read_status(team.res) == 0;
+    }
+    __syncthreads();
+    team.epoch += 1;
+    if (s_ok) {
+        st.a = s_st[0];
+        st.b = s_st[1];
+        st.Ka = s_st[2];
+        st.Kb = s_st[3];
+        st.L = s_st[4];
+        st.last_start = s_st[5];
+    }
+    return s_ok != 0;
+}
+
+// CTA 0 publishes the state and opens the gate.
+__device__ __forceinline__ void gate_open(Team& team, const LevelState& st)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        team.gs->st[0] = st.a;
+        team.gs->st[1] = st.b;
+        team.gs->st[2] = st.Ka;
+        team.gs->st[3] = st.Kb;
+        team.gs->st[4] = st.L;
+        team.gs->st[5] = st.last_start;
+        __threadfence();
+        st_release(&team.gs->epoch, team.epoch + 1);
+    }
+    __syncthreads();
+    team.epoch += 1;
+}
+
+// ---------------------------------------------------------------------------
+// One ordered BFS pass from `start` with pass key `base`.  Fills
+// rec[0..placed) and, when write_perm, the output.  Returns false if the team
+// must stop.  nlevels: number of levels; last_start: first position of the
+// last level.
 // ---------------------------------------------------------------------------
 template <int B, int EMAX>
-__device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsigned long long* agg, uint32_t start,
-                         bool sorted, bool write_perm, bool reverse, uint32_t& placed, uint32_t& nlevels,
-                         uint32_t& last_start)
+__device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsigned long long* agg,
+                         uint32_t& step, const Options& opt, uint32_t start, uint32_t base, bool sorted,
+                         bool write_perm, bool reverse, uint32_t& placed, uint32_t& nlevels, uint32_t& last_start)
 {
-    Chunk<B, EMAX> ch{s, M};
+    Chunk<B, EMAX> ch{s, M, base};
     const uint32_t t = threadIdx.x;
     const uint32_t G = team.size, R = team.rank;
     const uint32_t n = M.n;
 
-    // reset claims
-    for (uint64_t i = (uint64_t)R * B + t; i < n; i += (uint64_t)G * B)
-        M.claim[i] = kUnvisited;
-    if (!team.sync(1))
-        return false;
-
-    // seed the start (CTA 0 places it and claims its edges)
-    const uint32_t rs0 = ld_ro(M.rp + start), deg0 = ld_ro(M.rp + start + 1) - rs0;
+    LevelState st;
+    const uint4 sn = ld_node(M.node + start);
+    const uint32_t rs0 = sn.y, deg0 = sn.z;
+    st.a = 0;
+    st.b = 1;
+    st.Ka = 0;
+    st.Kb = deg0;
+    st.L = 0;
+    st.last_start = 0;
+    // CTA 0 places the start and claims its edges
     if (R == 0) {
         if (t == 0) {
-            atomicMin(M.claim + start, 0u);
+            atomicMax(&M.node[start].claim, base);
             __stcg(reinterpret_cast<uint4*>(M.rec), make_uint4(start, rs0, deg0, 0u));
             if (write_perm)
                 M.perm[reverse ? n - 1 : 0] = start;
@@ -693,35 +945,173 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsi
         for (uint32_t k = t; k < deg0; k += B) {
             const uint32_t d = ld_ro(M.ci + rs0 + k);
             if (PB_CHECK(M.res, d < n, 110))
-                atomicMin(M.claim + d, k + 1);
+                atomicMax(&M.node[d].claim, base - 1u - k);
         }
     }
-    if (!team.sync(2))
-        return false;
-
-    uint32_t a = 0, b = 1, Kb = deg0, Ka = 0;
-    uint32_t L = 0;
-    last_start = 0;
+    auto is_solo = [&](const LevelState& x) {
+        return G == 1 || ((x.b - x.a) <= opt.solo_parents && (x.Kb - x.Ka) <= opt.solo_edges);
+    };
+    bool solo = is_solo(st);
+    if (!solo) {
+        if (!team.sync(2))
+            return false;
+    }
     while (true) {
-        const uint32_t F = b - a;
-        // this CTA's parents
-        const uint32_t p_beg = a + (uint32_t)(((uint64_t)F * R) / G);
-        const uint32_t p_end = a + (uint32_t)(((uint64_t)F * (R + 1)) / G);
-        uint32_t tot_cnt = 0, tot_esum = 0;
-        if (G == 1) {
-            // collect and place chunk by chunk
-            uint32_t P = b, K = Kb;
-            uint32_t p = p_beg;
+        if (solo) {
+            // ---- CTA 0 alone: chunk by chunk with running offsets ----------
+            if (R == 0) {
+                while (true) {
+                    uint32_t P = st.b, K = st.Kb;
+                    uint32_t p = st.a;
+                    while (p < st.b) {
+                        const uint32_t used = ch.form(p, st.b);
+                        if (s.hub) {
+                            const uint32_t r0 = s.peb[0] - st.Ka;
+                            const Agg g = ch.hub_collect(r0, sorted);
+                            ch.hub_place_and_claim(r0, g.cnt, P, K, write_perm, reverse);
+                            P += g.cnt;
+                            K += g.esum;
+                        } else {
+                            const Agg g = ch.collect(sorted);
+                            ch.place_and_claim(P, K, write_perm, reverse);
+                            P += g.cnt;
+                            K += g.esum;
+                        }
+                        __syncthreads();
+                        p += used;
+                    }
+                    if (!team.block_ok())
+                        return false;
+                    const uint32_t tot = P - st.b;
+                    if (tot == 0) {
+                        st.a = st.b;  // an empty frontier marks the end of the pass
+                        break;
+                    }
+                    st.last_start = st.b;
+                    st.a = st.b;
+                    st.b = P;
+                    st.Ka = st.Kb;
+                    st.Kb = K;
+                    st.L += 1;
+                    if (st.b > n) {
+                        set_status(M.res, kErrCheck, 111);
+                        return false;
+                    }
+                    if (G > 1 && t == 0)
+                        atomicAdd(&team.gs->heartbeat, 1u);
+                    if (!is_solo(st))
+                        break;
+                }
+                if (G > 1)
+                    gate_open(team, st);
+            } else {
+                if (!gate_wait(team, st))
+                    return false;
+            }
+            if (st.a == st.b) {
+                // the pass ended during the solo run: every CTA leaves it
+                // together, so that none can still be reading this gate's
+                // state when CTA 0 opens the next one
+                if (G > 1 && !team.sync(8))
+                    return false;
+                break;
+            }
+            solo = false;
+            continue;
+        }
+        // ---- whole team ---------------------------------------------------
+        const uint32_t F = st.b - st.a;
+        const uint32_t p_beg = st.a + (uint32_t)(((uint64_t)F * R) / G);
+        const uint32_t p_end = st.a + (uint32_t)(((uint64_t)F * (R + 1)) / G);
+        // A1: collect and count
+        uint32_t my_cnt = 0, my_esum = 0, nunits = 0;
+        bool last_hub = false;
+        uint32_t p = p_beg;
+        while (p < p_end) {
+            const uint32_t used = ch.form(p, p_end);
+            Agg g;
+            last_hub = s.hub != 0;
+            if (last_hub)
+                g = ch.hub_collect(s.peb[0] - st.Ka, sorted);
+            else
+                g = ch.collect(sorted);
+            my_cnt += g.cnt;
+            my_esum += g.esum;
+            ++nunits;
+            p += used;
+            __syncthreads();
+        }
+        // publish (level-tagged), then prefetch while the others finish
+        ++step;
+        if (t == 0) {
+            st_relaxed64(agg + 2 * R, ((unsigned long long)step << 32) | my_cnt);
+            st_relaxed64(agg + 2 * R + 1, ((unsigned long long)step << 32) | my_esum);
+        }
+        const bool keep = nunits == 1 && !last_hub;
+        if (keep)
+            ch.prefetch();
+        // all-gather of the per-CTA totals
+        unsigned long long pre = 0, all = 0;
+        {
+            __shared__ int s_ok;
+            if (t == 0)
+                s_ok = 1;
+            __syncthreads();
+            for (uint32_t i = t; i < G; i += B) {
+                unsigned long long vc, ve;
+                unsigned long long t0 = 0;
+                uint32_t spins = 0;
+                while (true) {
+                    vc = ld_relaxed64(agg + 2 * i);
+                    ve = ld_relaxed64(agg + 2 * i + 1);
+                    if ((uint32_t)(vc >> 32) == step && (uint32_t)(ve >> 32) == step)
+                        break;
+                    if ((++spins & 31u) == 0) {
+                        if (read_status(M.res) != 0) {
+                            s_ok = 0;
+                            break;
+                        }
+                        const unsigned long long now = globaltimer();
+                        if (t0 == 0)
+                            t0 = now;
+                        else if (now - t0 > team.wait_ns) {
+                            set_status(M.res, kErrTimeout, 4);
+                            s_ok = 0;
+                            break;
+                        }
+                    }
+                    if (spins > 2048)
+                        __nanosleep(128);
+                }
+                const unsigned long long v = ((ve & 0xFFFFFFFFull) << 32) | (vc & 0xFFFFFFFFull);
+                all += v;
+                if (i < R)
+                    pre += v;
+            }
+            block_reduce_sum2<B>(pre, all, s.gat64);
+            if (!s_ok)
+                return false;
+        }
+        const uint32_t tot_cnt = (uint32_t)(all & 0xFFFFFFFFull);
+        const uint32_t tot_esum = (uint32_t)(all >> 32);
+        uint32_t P = st.b + (uint32_t)(pre & 0xFFFFFFFFull);
+        uint32_t K = st.Kb + (uint32_t)(pre >> 32);
+        // A2: place (the only unit is still in shared memory)
+        if (keep) {
+            ch.place_and_claim(P, K, write_perm, reverse);
+        } else if (nunits > 0) {
+            p = p_beg;
             while (p < p_end) {
                 const uint32_t used = ch.form(p, p_end);
                 if (s.hub) {
-                    const uint32_t r0 = s.peb[0] - Ka;
-                    Agg g = ch.hub_collect(r0, sorted);
-                    ch.hub_place_and_claim(r0, g.cnt, P, K, write_perm, reverse);
-                    P += g.cnt;
-                    K += g.esum;
+                    const uint32_t r0 = s.peb[0] - st.Ka;
+                    const uint32_t q = __ldcg(ch.hk1() + r0);
+                    const uint32_t qd = __ldcg(ch.hk1() + r0 + 1);
+                    ch.hub_place_and_claim(r0, q, P, K, write_perm, reverse);
+                    P += q;
+                    K += qd;
                 } else {
-                    Agg g = ch.collect(sorted);
+                    const Agg g = ch.collect(sorted);
                     ch.place_and_claim(P, K, write_perm, reverse);
                     P += g.cnt;
                     K += g.esum;
@@ -729,87 +1119,26 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsi
                 __syncthreads();
                 p += used;
             }
-            tot_cnt = P - b;
-            tot_esum = K - Kb;
-            if (!team.sync(3))
-                return false;
-        } else {
-            // A1: count
-            uint32_t my_cnt = 0, my_esum = 0, nunits = 0;
-            uint32_t p = p_beg;
-            while (p < p_end) {
-                const uint32_t used = ch.form(p, p_end);
-                Agg g;
-                if (s.hub)
-                    g = ch.hub_collect(s.peb[0] - Ka, sorted);
-                else
-                    g = ch.collect(sorted);
-                my_cnt += g.cnt;
-                my_esum += g.esum;
-                ++nunits;
-                p += used;
-                __syncthreads();
-            }
-            if (t == 0)
-                __stcg(agg + R, ((unsigned long long)my_esum << 32) | my_cnt);
-            if (!team.sync(4))
-                return false;
-            // prefix of the CTAs before this one, and the level total
-            unsigned long long pre = 0, all = 0;
-            for (uint32_t i = t; i < G; i += B) {
-                unsigned long long v = __ldcg(agg + i);
-                all += v;
-                if (i < R)
-                    pre += v;
-            }
-            pre = block_reduce_sum<B, unsigned long long>(pre, s.tmp64);
-            all = block_reduce_sum<B, unsigned long long>(all, s.tmp64);
-            tot_cnt = (uint32_t)(all & 0xFFFFFFFFull);
-            tot_esum = (uint32_t)(all >> 32);
-            uint32_t P = b + (uint32_t)(pre & 0xFFFFFFFFull);
-            uint32_t K = Kb + (uint32_t)(pre >> 32);
-            // A2: place (the last unit is still in shared memory if it was the only one)
-            if (nunits == 1 && !s.hub) {
-                ch.place_and_claim(P, K, write_perm, reverse);
-            } else {
-                p = p_beg;
-                while (p < p_end) {
-                    const uint32_t used = ch.form(p, p_end);
-                    if (s.hub) {
-                        const uint32_t r0 = s.peb[0] - Ka;
-                        const uint32_t q = __ldcg(ch.hk1() + r0);
-                        const uint32_t qd = __ldcg(ch.hk1() + r0 + 1);
-                        ch.hub_place_and_claim(r0, q, P, K, write_perm, reverse);
-                        P += q;
-                        K += qd;
-                    } else {
-                        Agg g = ch.collect(sorted);
-                        ch.place_and_claim(P, K, write_perm, reverse);
-                        P += g.cnt;
-                        K += g.esum;
-                    }
-                    __syncthreads();
-                    p += used;
-                }
-            }
-            if (!team.sync(5))
-                return false;
         }
+        if (!team.sync(5))
+            return false;
         if (tot_cnt == 0)
             break;
-        last_start = b;
-        a = b;
-        b += tot_cnt;
-        Ka = Kb;
-        Kb += tot_esum;
-        ++L;
-        if (b > n) {
-            set_status(M.res, kErrCheck, 111);
+        st.last_start = st.b;
+        st.a = st.b;
+        st.b += tot_cnt;
+        st.Ka = st.Kb;
+        st.Kb += tot_esum;
+        st.L += 1;
+        if (st.b > n) {
+            set_status(M.res, kErrCheck, 112);
             return false;
         }
+        solo = is_solo(st);
     }
-    placed = b;
-    nlevels = L + 1;
+    placed = st.b;
+    nlevels = st.L + 1;
+    last_start = st.last_start;
     return true;
 }
 
@@ -823,13 +1152,23 @@ __device__ __forceinline__ uint32_t next_peripheral_start(const MatrixView& M, u
     lo = max(lo, max(last_start, 1u));
     uint32_t best = 0, bestdeg = kUnvisited;
     for (uint32_t pos = lo; pos < n; ++pos) {
-        uint4 r = __ldcg(reinterpret_cast<const uint4*>(M.rec) + pos);
+        const uint4 r = __ldcg(reinterpret_cast<const uint4*>(M.rec) + pos);
         if (r.z <= bestdeg) {
             bestdeg = r.z;
             best = r.x;
         }
     }
     return best;
+}
+
+// Fills the node table (claim 0, row start, valence) of the matrix.
+template <int B>
+__device__ void init_nodes(const MatrixView& M, uint32_t R, uint32_t G)
+{
+    for (uint64_t v = (uint64_t)R * B + threadIdx.x; v < M.n; v += (uint64_t)G * B) {
+        const uint32_t a = ld_ro(M.rp + v), e = ld_ro(M.rp + v + 1);
+        __stcg(reinterpret_cast<uint4*>(M.node) + v, make_uint4(0u, a, e - a, 0u));
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -842,14 +1181,30 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
 {
     const uint32_t t = threadIdx.x;
     const uint32_t n = M.n;
+    const uint32_t G = team.size, R = team.rank;
     uint32_t start = opt.start;
     uint32_t passes = 0, ecc = 0, placed = 0, nlevels = 0, last_start = 0;
+    uint32_t step = 0;
 
     if (start != kUnvisited && start >= n) {
-        if (team.rank == 0 && t == 0)
+        if (R == 0 && t == 0)
             set_status(M.res, kErrArg, 2);
         return;
     }
+    init_nodes<B>(M, R, G);
+    if (!team.sync(1))
+        return;
+    // pass keys: pass p owns [p*kspan, p*kspan + nnz + 1]
+    const uint32_t kspan = M.nnz + 2u;
+    const uint32_t pmax = (uint32_t)(0xFFFFFFFFull / kspan) - 1u;
+    uint32_t pass_id = 0;
+    auto reset_claims = [&]() -> bool {
+        for (uint64_t v = (uint64_t)R * B + t; v < n; v += (uint64_t)G * B)
+            M.node[v].claim = 0u;
+        pass_id = 0;
+        return team.sync(7);
+    };
+
     if (n == 1) {
         // one node: the start search runs one pass and records nothing
         passes = start == kUnvisited ? 1 : 0;
@@ -860,10 +1215,15 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
         uint32_t lastdist = 0;
         while (true) {
             ++passes;
-            if (!bfs_pass<B, EMAX>(s, M, team, agg, start, false, false, false, placed, nlevels, last_start))
+            if (pass_id + 1 > pmax && !reset_claims())
+                return;
+            ++pass_id;
+            const uint32_t base = pass_id * kspan + M.nnz + 1u;
+            if (!bfs_pass<B, EMAX>(s, M, team, agg, step, opt, start, base, false, false, false, placed, nlevels,
+                                   last_start))
                 return;
             if (placed != n) {
-                if (team.rank == 0 && t == 0)
+                if (R == 0 && t == 0)
                     set_status(M.res, kErrDisconnected, 0);
                 return;
             }
@@ -873,7 +1233,7 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
                 break;
             }
             if (passes > n) {  // eccentricities only grow; cannot happen on a valid run
-                if (team.rank == 0 && t == 0)
+                if (R == 0 && t == 0)
                     set_status(M.res, kErrCheck, 3);
                 return;
             }
@@ -886,7 +1246,7 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
         }
     }
     if (opt.mode == kModeStartOnly) {
-        if (team.rank == 0 && t == 0) {
+        if (R == 0 && t == 0) {
             M.res->start = start;
             M.res->passes = passes;
             M.res->ecc = ecc;
@@ -895,10 +1255,15 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
         return;
     }
     // the final, degree-sorted pass writes the permutation
-    if (!bfs_pass<B, EMAX>(s, M, team, agg, start, true, true, opt.reverse != 0, placed, nlevels, last_start))
+    if (pass_id + 1 > pmax && !reset_claims())
+        return;
+    ++pass_id;
+    const uint32_t base = pass_id * kspan + M.nnz + 1u;
+    if (!bfs_pass<B, EMAX>(s, M, team, agg, step, opt, start, base, true, true, opt.reverse != 0, placed, nlevels,
+                           last_start))
         return;
     if (placed != n) {
-        if (team.rank == 0 && t == 0) {
+        if (R == 0 && t == 0) {
             set_status(M.res, kErrDisconnected, 1);
             M.res->placed = placed;
         }
@@ -906,11 +1271,10 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
     }
 
     if (opt.want_bw) {
-        const uint32_t G = team.size, R = team.rank;
-        // inverse permutation (CM positions) into claim[]
+        // inverse permutation (CM positions) into node[].inv
         for (uint64_t pos = (uint64_t)R * B + t; pos < n; pos += (uint64_t)G * B) {
-            uint4 r = __ldcg(reinterpret_cast<const uint4*>(M.rec) + pos);
-            M.claim[r.x] = (uint32_t)pos;
+            const uint4 r = __ldcg(reinterpret_cast<const uint4*>(M.rec) + pos);
+            M.node[r.x].inv = (uint32_t)pos;
         }
         if (!team.sync(6))
             return;
@@ -919,31 +1283,28 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
             const uint32_t a = ld_ro(M.rp + i), e = ld_ro(M.rp + i + 1);
             if (a == e)
                 continue;
-            const uint32_t me = __ldcg(M.claim + i);
-            uint32_t mn = me, mx = me, mnr = kUnvisited, mxr = 0;
+            const uint32_t me = __ldcg(&M.node[i].inv);
+            uint32_t mnr = kUnvisited, mxr = 0;
             for (uint32_t k = a; k < e; ++k) {
-                const uint32_t p = __ldcg(M.claim + ld_ro(M.ci + k));
+                const uint32_t p = __ldcg(&M.node[ld_ro(M.ci + k)].inv);
                 mnr = min(mnr, p);
                 mxr = max(mxr, p);
             }
-            mn = min(mn, mnr);
-            mx = max(mx, mxr);
             // computeBandwidth (main.cpp:143-184): max(row - min, max - row), >= 0
             const unsigned long long b1 = me >= mnr ? (unsigned long long)(me - mnr) : 0ull;
             const unsigned long long b2 = mxr >= me ? (unsigned long long)(mxr - me) : 0ull;
             bw = max(bw, max(b1, b2));
-            // profile of the CM order and of its reverse
-            plo += (unsigned long long)(me - mn);
-            phi += (unsigned long long)(mx - me);
+            // profile of the CM order (row - min col) and of its reverse (max col - row)
+            plo += b1;
+            phi += b2;
             // initial bandwidth: first / last stored column (main.cpp:114-129)
             const uint32_t c0 = ld_ro(M.ci + a), c1 = ld_ro(M.ci + e - 1);
-            unsigned long long i0 = i >= c0 ? i - c0 : 0, i1 = c1 >= i ? c1 - i : 0;
+            const unsigned long long i0 = i >= c0 ? i - c0 : 0, i1 = c1 >= i ? c1 - i : 0;
             bw0 = max(bw0, max(i0, i1));
         }
         bw = block_reduce_max<B, unsigned long long>(bw, s.tmp64);
         bw0 = block_reduce_max<B, unsigned long long>(bw0, s.tmp64);
-        plo = block_reduce_sum<B, unsigned long long>(plo, s.tmp64);
-        phi = block_reduce_sum<B, unsigned long long>(phi, s.tmp64);
+        block_reduce_sum2<B>(plo, phi, s.tmp64);
         if (t == 0) {
             atomicMax(&M.res->bandwidth, bw);
             atomicMax(&M.res->initial_bw, bw0);
@@ -951,7 +1312,7 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
             atomicAdd(&M.res->profile_hi, phi);
         }
     }
-    if (team.rank == 0 && t == 0) {
+    if (R == 0 && t == 0) {
         M.res->start = start;
         M.res->passes = passes;
         M.res->ecc = ecc;

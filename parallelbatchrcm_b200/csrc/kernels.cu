@@ -4,9 +4,14 @@
 //                     and the largest valence (decides whether hub scratch is
 //                     needed); a bad CSR never reaches the engine.
 //   k_reorder_team    one matrix, all CTAs of a cooperative launch: start
-//                     search + CM pass + reverse + bandwidth in one launch.
-//   k_reorder_batch   many matrices, one CTA per matrix, matrices handed out
-//                     by an atomic counter (largest first).
+//                     search + CM pass + reverse + bandwidth in one launch
+//                     (agg: 2 words per CTA for the level all-gather, then
+//                     one barrier flag word per CTA + phantom; all zeroed
+//                     before the launch together with the GridSync words).
+//   k_reorder_batch   many matrices in one cooperative launch: a work list of
+//                     (job, team rank) slots handed out by an atomic counter,
+//                     biggest jobs first; small matrices run on one CTA, big
+//                     ones on a team of CTAs with their own barrier words.
 //   k_bandwidth_*     bandwidth / profile of a caller permutation.
 #include <algorithm>
 #include <cstdio>
@@ -60,10 +65,10 @@ __global__ void __launch_bounds__(256) k_validate(const uint32_t* __restrict__ r
 }
 
 // one CTA per matrix
-__global__ void __launch_bounds__(256) k_validate_batch(const MatrixView* jobs, uint32_t njobs)
+__global__ void __launch_bounds__(256) k_validate_batch(const BatchJob* jobs, uint32_t njobs)
 {
     for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
-        const MatrixView M = jobs[j];
+        const MatrixView M = jobs[j].M;
         validate_one(M.rp, M.ci, M.n, M.nnz, M.res, threadIdx.x, blockDim.x);
         __syncthreads();
     }
@@ -95,18 +100,26 @@ __global__ void __launch_bounds__(B, 1) k_reorder_team(MatrixView M, Options opt
         return;
     Team team;
     team.gs = gridDim.x > 1 ? gs : nullptr;
+    team.flags = reinterpret_cast<unsigned int*>(agg + 2 * gridDim.x);
     team.size = gridDim.x;
     team.rank = blockIdx.x;
     team.expected = gridDim.x + opt.phantom;
-    team.gen = 0;
+    team.mode = opt.barrier;
+    team.target = 0;
+    team.epoch = 0;
     team.wait_ns = opt.wait_ns;
     team.res = M.res;
     reorder_matrix<B, EMAX>(s, M, team, agg, opt);
 }
 
+// Many matrices in one launch.  Every CTA takes the next slot of the work
+// list; a slot names a job and this CTA's rank in the job's team.  Teams are
+// formed from consecutive slots, biggest jobs first; the launch is
+// cooperative, so every CTA is resident and a team's members that joined
+// first only wait (bounded) for the next CTAs that free up.
 template <int B, int EMAX>
-__global__ void __launch_bounds__(B) k_reorder_batch(const MatrixView* jobs, uint32_t njobs, uint32_t* counter,
-                                                     Options opt)
+__global__ void __launch_bounds__(B) k_reorder_batch(const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots,
+                                                     uint32_t* counter, Options opt)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     auto& s = *reinterpret_cast<Smem<B, EMAX>*>(smem_raw);
@@ -114,22 +127,26 @@ __global__ void __launch_bounds__(B) k_reorder_batch(const MatrixView* jobs, uin
         if (threadIdx.x == 0)
             s.bcast[7] = atomicAdd(counter, 1u);
         __syncthreads();
-        const uint32_t j = s.bcast[7];
+        const uint32_t slot = s.bcast[7];
         __syncthreads();
-        if (j >= njobs)
+        if (slot >= nslots)
             break;
-        const MatrixView M = jobs[j];
-        if (skip_matrix<EMAX>(M, threadIdx.x == 0))
+        const BatchSlot sl = slots[slot];
+        const BatchJob job = jobs[sl.job];
+        if (skip_matrix<EMAX>(job.M, sl.rank == 0 && threadIdx.x == 0))
             continue;
         Team team;
-        team.gs = nullptr;
-        team.size = 1;
-        team.rank = 0;
-        team.expected = 1;
-        team.gen = 0;
+        team.gs = job.team > 1 ? job.gs : nullptr;
+        team.flags = job.team > 1 ? reinterpret_cast<unsigned int*>(job.words + 2 * job.team) : nullptr;
+        team.size = job.team;
+        team.rank = sl.rank;
+        team.expected = job.team;
+        team.mode = 0;
+        team.target = 0;
+        team.epoch = 0;
         team.wait_ns = opt.wait_ns;
-        team.res = M.res;
-        reorder_matrix<B, EMAX>(s, M, team, nullptr, opt);
+        team.res = job.M.res;
+        reorder_matrix<B, EMAX>(s, job.M, team, job.words, opt);
         __syncthreads();
     }
 }
@@ -149,7 +166,7 @@ __global__ void __launch_bounds__(256) k_bw_inverse(const uint32_t* __restrict__
 __global__ void __launch_bounds__(256) k_bw_rows(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
                                                  uint32_t n, const uint32_t* __restrict__ inv, DevResult* res)
 {
-    __shared__ unsigned long long tmp[9];
+    __shared__ unsigned long long tmp[18];
     unsigned long long bw = 0, bw0 = 0, plo = 0, phi = 0;
     if (read_status(res) == 0) {
         for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -176,8 +193,7 @@ __global__ void __launch_bounds__(256) k_bw_rows(const uint32_t* __restrict__ rp
     }
     bw = block_reduce_max<256, unsigned long long>(bw, tmp);
     bw0 = block_reduce_max<256, unsigned long long>(bw0, tmp);
-    plo = block_reduce_sum<256, unsigned long long>(plo, tmp);
-    phi = block_reduce_sum<256, unsigned long long>(phi, tmp);
+    block_reduce_sum2<256>(plo, phi, tmp);
     if (threadIdx.x == 0) {
         atomicMax(&res->bandwidth, bw);
         atomicMax(&res->initial_bw, bw0);
@@ -237,14 +253,25 @@ struct Variant {
         return cudaLaunchCooperativeKernel((const void*)k_reorder_team<B, EMAX>, dim3(ctas), dim3(B), args, smem(),
                                            st);
     }
-    static cudaError_t batch(const MatrixView* jobs, uint32_t njobs, uint32_t* counter, const Options& opt, int ctas,
-                             cudaStream_t st)
+    static cudaError_t batch(const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
+                             const Options& opt, int ctas, bool cooperative, cudaStream_t st)
     {
         cudaError_t e = prepare();
         if (e != cudaSuccess)
             return e;
-        k_reorder_batch<B, EMAX><<<ctas, B, smem(), st>>>(jobs, njobs, counter, opt);
-        return cudaGetLastError();
+        if (!cooperative) {
+            // no team: CTAs never wait for each other, a plain launch will do
+            k_reorder_batch<B, EMAX><<<ctas, B, smem(), st>>>(jobs, slots, nslots, counter, opt);
+            return cudaGetLastError();
+        }
+        const BatchJob* j = jobs;
+        const BatchSlot* sl = slots;
+        uint32_t ns = nslots;
+        uint32_t* c = counter;
+        Options o = opt;
+        void* args[] = {&j, &sl, &ns, &c, &o};
+        return cudaLaunchCooperativeKernel((const void*)k_reorder_batch<B, EMAX>, dim3(ctas), dim3(B), args, smem(),
+                                           st);
     }
 };
 
@@ -289,10 +316,10 @@ cudaError_t launch_team(int v, const MatrixView& M, const Options& opt, GridSync
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_batch(int v, const MatrixView* jobs, uint32_t njobs, uint32_t* counter, const Options& opt,
-                         int ctas, cudaStream_t st)
+cudaError_t launch_batch(int v, const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
+                         const Options& opt, int ctas, bool cooperative, cudaStream_t st)
 {
-    PBRCM_DISPATCH(v, batch(jobs, njobs, counter, opt, ctas, st));
+    PBRCM_DISPATCH(v, batch(jobs, slots, nslots, counter, opt, ctas, cooperative, st));
     return cudaErrorInvalidValue;
 }
 
@@ -307,7 +334,7 @@ cudaError_t launch_validate(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_validate_batch(const MatrixView* jobs, uint32_t njobs, int sms, cudaStream_t st)
+cudaError_t launch_validate_batch(const BatchJob* jobs, uint32_t njobs, int sms, cudaStream_t st)
 {
     int blocks = (int)std::min<uint32_t>(njobs, (uint32_t)sms * 8);
     if (blocks < 1)

@@ -20,15 +20,16 @@ extern const VariantInfo kVariants[kNumVariants];
 
 size_t variant_smem(int v);
 int team_max_ctas(int v, int sms);   // co-resident CTAs of the team kernel
-int batch_max_ctas(int v, int sms);  // resident CTAs of the batch kernel
+int batch_max_ctas(int v, int sms);  // co-resident CTAs of the batch kernel
 
 cudaError_t launch_validate(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint32_t nnz, DevResult* res,
                             int sms, cudaStream_t st);
-cudaError_t launch_validate_batch(const MatrixView* jobs, uint32_t njobs, int sms, cudaStream_t st);
+cudaError_t launch_validate_batch(const BatchJob* jobs, uint32_t njobs, int sms, cudaStream_t st);
 cudaError_t launch_team(int v, const MatrixView& M, const Options& opt, GridSync* gs, unsigned long long* agg,
                         int ctas, cudaStream_t st);
-cudaError_t launch_batch(int v, const MatrixView* jobs, uint32_t njobs, uint32_t* counter, const Options& opt,
-                         int ctas, cudaStream_t st);
+// cooperative: required when some job has a team of more than one CTA
+cudaError_t launch_batch(int v, const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
+                         const Options& opt, int ctas, bool cooperative, cudaStream_t st);
 cudaError_t launch_bandwidth(const uint32_t* rp, const uint32_t* ci, uint32_t n, const uint32_t* perm, uint32_t* inv,
                              DevResult* res, int sms, cudaStream_t st);
 

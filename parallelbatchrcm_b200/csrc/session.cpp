@@ -85,9 +85,10 @@ struct Request {
     unsigned char* host = nullptr;
     size_t host_cap = 0;
     size_t off_rp = 0, off_ci = 0, off_view = 0, off_perm = 0, off_res = 0;
-    // device block: [rp | ci | claim | rec | perm | res | gs | counter | hub?]
+    // device block: [rp | ci | node | rec | perm | res | gs | counter + view | agg | hub?]
     unsigned char* dev = nullptr;
-    size_t d_rp = 0, d_ci = 0, d_claim = 0, d_rec = 0, d_perm = 0, d_res = 0, d_gs = 0, d_cnt = 0, d_hub = 0;
+    size_t d_rp = 0, d_ci = 0, d_node = 0, d_rec = 0, d_perm = 0, d_res = 0, d_gs = 0, d_cnt = 0, d_agg = 0,
+           d_hub = 0;
     bool team = false;
     int stream = 0;
     cudaEvent_t ev = nullptr;
@@ -131,15 +132,15 @@ struct pbrcm_session {
 
 namespace {
 
-size_t device_bytes(uint32_t n, uint64_t nnz, bool hub, size_t* offs)
+size_t device_bytes(uint32_t n, uint64_t nnz, bool hub, int team_ctas, size_t* offs)
 {
     size_t o = 0;
     offs[0] = o;  // rp
     o = align16(o + 4 * ((size_t)n + 1));
     offs[1] = o;  // ci
     o = align16(o + 4 * (size_t)nnz);
-    offs[2] = o;  // claim
-    o = align16(o + 4 * (size_t)n);
+    offs[2] = o;  // node table
+    o = align16(o + 16 * (size_t)n);
     offs[3] = o;  // rec
     o = align16(o + 16 * (size_t)n);
     offs[4] = o;  // perm
@@ -148,9 +149,11 @@ size_t device_bytes(uint32_t n, uint64_t nnz, bool hub, size_t* offs)
     o = align16(o + sizeof(DevResult));
     offs[6] = (o + 127) & ~(size_t)127;  // gs
     o = offs[6] + sizeof(GridSync);
-    offs[7] = o;  // counter (+ job view)
-    o = align16(o + 16 + sizeof(MatrixView));
-    offs[8] = o;  // hub
+    offs[7] = o;  // counter, then one BatchJob and one BatchSlot
+    o = align16(o + 16 + sizeof(BatchJob) + sizeof(BatchSlot));
+    offs[8] = o;  // agg (2 words per team CTA)
+    o = align16(o + team_words_bytes(team_ctas));
+    offs[9] = o;  // hub
     if (hub)
         o = align16(o + 16 * std::max<uint64_t>(nnz, 1));
     return o;
@@ -170,15 +173,21 @@ bool pbrcm_session::launch(Request* r)
     M.ci = reinterpret_cast<const uint32_t*>(D + r->d_ci);
     M.n = r->n;
     M.nnz = (uint32_t)r->nnz;
-    M.claim = reinterpret_cast<uint32_t*>(D + r->d_claim);
+    M.node = reinterpret_cast<NodeEntry*>(D + r->d_node);
     M.rec = reinterpret_cast<PosRec*>(D + r->d_rec);
     M.perm = reinterpret_cast<uint32_t*>(D + r->d_perm);
     M.hub = r->team && r->maxdeg > (uint32_t)kVariants[c.team_variant].emax
                 ? reinterpret_cast<uint32_t*>(D + r->d_hub)
                 : nullptr;
     M.res = reinterpret_cast<DevResult*>(D + r->d_res);
-    std::memcpy(r->host + r->off_view, &M, sizeof(M));
-    MatrixView* d_view = reinterpret_cast<MatrixView*>(D + r->d_cnt + 16);
+    BatchJob J{};
+    J.M = M;
+    J.team = 1;
+    const BatchSlot one{0, 0};
+    std::memcpy(r->host + r->off_view, &J, sizeof(J));
+    std::memcpy(r->host + r->off_view + sizeof(J), &one, sizeof(one));
+    BatchJob* d_job = reinterpret_cast<BatchJob*>(D + r->d_cnt + 16);
+    BatchSlot* d_slot = reinterpret_cast<BatchSlot*>(D + r->d_cnt + 16 + sizeof(BatchJob));
     uint32_t* d_counter = reinterpret_cast<uint32_t*>(D + r->d_cnt);
     bool ok = cudaMemcpyAsync(D + r->d_rp, r->host + r->off_rp, 4 * ((size_t)r->n + 1), cudaMemcpyHostToDevice,
                               st) == cudaSuccess;
@@ -186,17 +195,18 @@ bool pbrcm_session::launch(Request* r)
         ok = ok && cudaMemcpyAsync(D + r->d_ci, r->host + r->off_ci, 4 * (size_t)r->nnz, cudaMemcpyHostToDevice,
                                    st) == cudaSuccess;
     ok = ok && cudaMemsetAsync(D + r->d_res, 0, sizeof(DevResult), st) == cudaSuccess;
-    ok = ok && cudaMemsetAsync(D + r->d_gs, 0, sizeof(GridSync) + 0, st) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(D + r->d_gs, 0, sizeof(GridSync), st) == cudaSuccess;
+    if (r->team)
+        ok = ok && cudaMemsetAsync(D + r->d_agg, 0, team_words_bytes(team_ctas), st) == cudaSuccess;
     ok = ok && cudaMemsetAsync(d_counter, 0, 16, st) == cudaSuccess;
-    ok = ok && cudaMemcpyAsync(d_view, r->host + r->off_view, sizeof(MatrixView), cudaMemcpyHostToDevice, st) ==
-                   cudaSuccess;
+    ok = ok && cudaMemcpyAsync(d_job, r->host + r->off_view, sizeof(BatchJob) + sizeof(BatchSlot),
+                               cudaMemcpyHostToDevice, st) == cudaSuccess;
     ok = ok && launch_validate(M.rp, M.ci, M.n, M.nnz, M.res, c.sms, st) == cudaSuccess;
     if (r->team)
         ok = ok && launch_team(c.team_variant, M, r->opt, reinterpret_cast<GridSync*>(D + r->d_gs),
-                               reinterpret_cast<unsigned long long*>(c.d_agg_session_slot(r->stream)), team_ctas,
-                               st) == cudaSuccess;
+                               reinterpret_cast<unsigned long long*>(D + r->d_agg), team_ctas, st) == cudaSuccess;
     else
-        ok = ok && launch_batch(small_variant, d_view, 1, d_counter, r->opt, 1, st) == cudaSuccess;
+        ok = ok && launch_batch(small_variant, d_job, d_slot, 1, d_counter, r->opt, 1, false, st) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(r->host + r->off_perm, M.perm, 4 * (size_t)r->n, cudaMemcpyDeviceToHost, st) ==
                    cudaSuccess;
     ok = ok && cudaMemcpyAsync(r->host + r->off_res, M.res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) ==
@@ -268,29 +278,6 @@ void pbrcm_session::run()
     }
 }
 
-// The team kernel needs a per-stream aggregate array; it lives in the context.
-namespace pbrcm {
-unsigned long long* Context::d_agg_session_slot(int s)
-{
-    const int maxc = team_max_ctas(team_variant, sms);
-    const size_t need = (size_t)(s + 1) * (size_t)std::max(maxc, 1);
-    if (need > cap_agg_session) {
-        // grown only from the worker before any launch on stream s is in flight
-        unsigned long long* p = nullptr;
-        const size_t want = (size_t)64 * (size_t)std::max(maxc, 1);
-        if (cudaMalloc(&p, sizeof(unsigned long long) * want) != cudaSuccess)
-            return nullptr;
-        if (d_agg_session) {
-            cudaDeviceSynchronize();
-            cudaFree(d_agg_session);
-        }
-        d_agg_session = p;
-        cap_agg_session = want;
-    }
-    return d_agg_session + (size_t)s * (size_t)std::max(maxc, 1);
-}
-}  // namespace pbrcm
-
 extern "C" {
 
 int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg, pbrcm_session** out)
@@ -323,11 +310,6 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
     }
     uint64_t thr = ~0ull;
     cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &thr);
-    // the agg slots must exist before any team launch
-    if (!s->C->d_agg_session_slot((int)ns - 1)) {
-        delete s;
-        return PBRCM_ERR_OOM;
-    }
     s->worker = std::thread([s] { s->run(); });
     *out = s;
     return PBRCM_OK;
@@ -363,7 +345,7 @@ void pbrcm_session_destroy(pbrcm_session* s)
 int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const uint32_t* col_idx, uint32_t n,
                              uint64_t nnz, const pbrcm_options* opts, uint64_t* ticket)
 {
-    if (!s || !row_ptr || (!col_idx && nnz) || !ticket || n == 0 || n == 0xFFFFFFFFu || nnz >= 0xFFFFFFFFull)
+    if (!s || !row_ptr || (!col_idx && nnz) || !ticket || n == 0 || n == 0xFFFFFFFFu || nnz > kMaxNnz)
         return PBRCM_ERR_ARG;
     auto* r = new (std::nothrow) Request();
     if (!r)
@@ -371,6 +353,7 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     r->n = n;
     r->nnz = nnz;
     r->opt = make_options(opts, kModeFull);
+    apply_team_shape(*s->C, r->opt);
     r->opt.phantom = 0;
     uint32_t maxdeg = 0;
     for (uint32_t i = 0; i < n; ++i)
@@ -378,17 +361,19 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     r->maxdeg = maxdeg;
     const int emax_small = kVariants[s->small_variant].emax;
     r->team = n > s->team_cutoff_n || maxdeg > (uint32_t)emax_small;
-    size_t offs[9];
-    r->dev_bytes = device_bytes(n, nnz, r->team && maxdeg > (uint32_t)kVariants[s->C->team_variant].emax, offs);
+    size_t offs[10];
+    r->dev_bytes = device_bytes(n, nnz, r->team && maxdeg > (uint32_t)kVariants[s->C->team_variant].emax,
+                                s->team_ctas, offs);
     r->d_rp = offs[0];
     r->d_ci = offs[1];
-    r->d_claim = offs[2];
+    r->d_node = offs[2];
     r->d_rec = offs[3];
     r->d_perm = offs[4];
     r->d_res = offs[5];
     r->d_gs = offs[6];
     r->d_cnt = offs[7];
-    r->d_hub = offs[8];
+    r->d_agg = offs[8];
+    r->d_hub = offs[9];
     if (r->dev_bytes > s->cap_bytes) {
         delete r;
         return PBRCM_ERR_BUSY;
@@ -399,7 +384,7 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     r->off_ci = o;
     o = align16(o + 4 * (size_t)nnz);
     r->off_view = o;
-    o = align16(o + sizeof(MatrixView));
+    o = align16(o + sizeof(BatchJob) + sizeof(BatchSlot));
     r->off_perm = o;
     o = align16(o + 4 * (size_t)n);
     r->off_res = o;

@@ -1,6 +1,7 @@
 // types.h -- plain data shared by the engine's device code and host code.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 
 namespace pbrcm {
@@ -17,16 +18,33 @@ enum : uint32_t {
     kNeedHub = 100,  // internal: relaunch with hub scratch
 };
 
-// One record per queue position: node, row start, valence, edge base.
+// One record per queue position: node, row start, valence, edge id base.
 struct alignas(16) PosRec {
     uint32_t node, rs, deg, ebase;
 };
 
-// Grid barrier state: reset to zero before every cooperative launch.
+// One entry per node: claim key (see engine.cuh), row start, valence and,
+// after the final pass, the node's position (inverse permutation).  Claim,
+// row start and valence share one 16-byte load.
+struct alignas(16) NodeEntry {
+    uint32_t claim, rs, deg, inv;
+};
+
+// Grid-team synchronisation words, zeroed before every cooperative launch.
+//   count      monotonic barrier counter: every CTA adds 1 per barrier and
+//              waits until it reaches (barriers so far) x (team size)
+//   epoch      bumped by CTA 0 when it hands a run of small levels ("solo"
+//              levels it processed alone) back to the whole team
+//   heartbeat  bumped by CTA 0 once per solo level (keeps the waiters' bounded
+//              wait from running out while CTA 0 makes progress)
+//   st[]       the level state CTA 0 publishes with the epoch
 struct alignas(128) GridSync {
-    unsigned int arrive;
-    unsigned int gen;
-    unsigned int pad[30];
+    unsigned int count;
+    unsigned int pad0[31];
+    unsigned int epoch;
+    unsigned int heartbeat;
+    unsigned int st[14];
+    unsigned int pad1[16];
 };
 
 // Device-side result of one matrix.
@@ -50,12 +68,37 @@ struct MatrixView {
     const uint32_t* __restrict__ rp;   // n+1
     const uint32_t* __restrict__ ci;   // nnz
     uint32_t n;
-    uint32_t nnz;                      // < 2^32 - 1 (checked by the host)
-    uint32_t* claim;                   // n   (reused as the inverse permutation)
+    uint32_t nnz;                      // <= kMaxNnz (checked by the host)
+    NodeEntry* node;                   // n
     PosRec* rec;                       // n
     uint32_t* perm;                    // n   output
     uint32_t* hub;                     // 4 * nnz hub scratch, or nullptr if no hub can occur
     DevResult* res;
+};
+
+constexpr uint64_t kMaxNnz = 0xFFFFFFF0ull;
+
+// Bytes of the per-launch team words of a cooperative launch of `ctas` CTAs:
+// 2 x u64 per CTA for the level all-gather, then one u32 barrier flag per
+// CTA (plus room for the phantom test CTA).
+inline size_t team_words_bytes(int ctas)
+{
+    return 16 * (size_t)(ctas > 0 ? ctas : 1) + 4 * ((size_t)(ctas > 0 ? ctas : 1) + 8);
+}
+
+// One matrix of a batch: its view, its team size (CTAs that reorder it
+// together) and, for teams, its own barrier words.
+struct BatchJob {
+    MatrixView M;
+    uint32_t team;
+    uint32_t pad;
+    GridSync* gs;                 // team > 1: zeroed GridSync of this job
+    unsigned long long* words;    // team > 1: zeroed team_words_bytes(team)
+};
+
+// One entry of the batch work list: member `rank` of job `job`'s team.
+struct BatchSlot {
+    uint32_t job, rank;
 };
 
 struct Options {
@@ -66,6 +109,10 @@ struct Options {
     unsigned long long wait_ns;
     uint32_t phantom;       // extra CTAs a grid barrier waits for (test hook)
     uint32_t mode;          // kModeFull, or kModeStartOnly: stop after the start search
+    uint32_t solo_edges;    // a level with at most this many edges runs on CTA 0 alone
+    uint32_t solo_parents;  // ... and at most this many parents
+    uint32_t barrier;       // team barrier: 0 counter, 1 flag array
+    uint32_t pad;
 };
 
 constexpr uint32_t kModeFull = 0;
