@@ -144,14 +144,17 @@ def measured_peak():
 
 
 def profile_traffic():
-    """dram bytes per launch of the team kernel from the committed ncu summary,
-    scaled to the full workload (profiles/k_reorder_team_grid3d.json)."""
-    p = os.path.join(ROOT, "profiles", "k_reorder_team_grid3d.json")
+    """dram__bytes_read.sum + dram__bytes_write.sum of one team-kernel launch on
+    this workload, from the committed ncu summary
+    (profiles/k_reorder_team_grid3d_128.md), or None."""
+    p = os.path.join(ROOT, "profiles", "k_reorder_team_grid3d_128.md")
     if not os.path.exists(p):
         return None
     with open(p) as f:
-        d = json.load(f)
-    return d.get("dram_bytes_per_launch_full")
+        for line in f:
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":")[1])
+    return None
 
 
 def algorithmic_bytes(n: int, nnz: int, passes: int) -> int:
