@@ -151,6 +151,25 @@ PBRCM_API int32_t pbrcm_bandwidth(pbrcm_context* ctx, const uint32_t* row_ptr, c
                         uint32_t n, uint64_t nnz, const uint32_t* perm, int64_t* bandwidth,
                         int64_t* initial_bandwidth, uint64_t* profile);
 
+/*
+ * One full reorder of a DEVICE-resident matrix that allocates nothing.  No
+ * counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc while they run (a host application whose device memory is
+ * owned by its own pool or by a budget fixed at start-up, or code that must
+ * not let an allocation synchronise the device mid-flight).  All scratch
+ * lives in a static device array reserved when the library is loaded (about
+ * 32 MiB on every GPU that loads it, held until exit).  Limits: n <= 2^20
+ * nodes and no row longer than 1024 entries; larger inputs return
+ * PBRCM_ERR_ARG.  The first call on a device looks up the array's address and
+ * should come before any stream capture.  Every call shares the array, so
+ * calls that overlap on the GPU race: serialise them.  Same options, result
+ * and permutation as pbrcm_reorder_device; synchronises `stream` (a
+ * cudaStream_t, NULL = the legacy default stream) before returning.
+ */
+PBRCM_API int32_t pbrcm_reorder_device_noalloc(const uint32_t* d_row_ptr, const uint32_t* d_col_idx, uint32_t n,
+                                               uint64_t nnz, const pbrcm_options* opts, uint32_t* d_perm_out,
+                                               pbrcm_result* result, void* stream);
+
 /* ---------------------------------------------------------------------- */
 /* Many matrices in one persistent launch.                                 */
 /* ---------------------------------------------------------------------- */

@@ -81,6 +81,8 @@ SIGNATURES = {
     "pbrcm_reorder": (_i32, [_vp, _vp, _vp, _u32, _u64, ctypes.POINTER(Options), _vp, ctypes.POINTER(Result)]),
     "pbrcm_reorder_device": (_i32, [_vp, _vp, _vp, _u32, _u64, ctypes.POINTER(Options), _vp,
                                     ctypes.POINTER(Result), _vp]),
+    "pbrcm_reorder_device_noalloc": (_i32, [_vp, _vp, _u32, _u64, ctypes.POINTER(Options), _vp,
+                                            ctypes.POINTER(Result), _vp]),
     "pbrcm_find_peripheral": (_i32, [_vp, _vp, _vp, _u32, _u64, _pu32, _pu32, _pu32]),
     "pbrcm_bandwidth": (_i32, [_vp, _vp, _vp, _u32, _u64, _vp, ctypes.POINTER(ctypes.c_int64),
                                ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_uint64)]),

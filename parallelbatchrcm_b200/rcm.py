@@ -30,7 +30,8 @@ from . import _lib
 from ._lib import AUTO_START, DEBUG_PHANTOM_CTA, Matrix, Options, Result, SessionConfig, SessionStats
 
 __all__ = [
-    "PbrcmError", "Context", "default_options", "reorder", "reorder_device", "find_peripheral",
+    "PbrcmError", "Context", "default_options", "reorder", "reorder_device", "reorder_device_noalloc",
+    "find_peripheral",
     "bandwidth", "reorder_batch", "reorder_batch_device", "Session", "load_mtx", "prepare_csr",
     "Graph", "GPU_BATCH", "SimplePeripheral", "compute_bandwidth", "check_bandwidth", "max_valency",
     "check_permutation", "AUTO_START", "DEBUG_PHANTOM_CTA",
@@ -144,6 +145,31 @@ def reorder_device(row_ptr_t, col_idx_t, perm_t=None, *, reverse: bool = True, s
     d = res.as_dict()
     d["rc"] = rc
     return perm_t, d
+
+
+def reorder_device_noalloc(row_ptr_t, col_idx_t, perm_t, *, reverse: bool = True, start: int | None = None,
+                           want_bandwidth: bool = True, stream=None, raise_on_error: bool = True, **opt_kw):
+    """Full reorder of a device-resident CSR that allocates no device memory
+    (pbrcm_reorder_device_noalloc): for callers that cannot allocate while
+    they run.  perm_t (n int32/uint32 on the GPU) receives the permutation.
+    At most 2^20 nodes and rows of at most 1024 entries; calls that overlap on
+    the GPU race on the shared scratch, so serialise them.  Returns the
+    result dict."""
+    import torch
+
+    n = row_ptr_t.numel() - 1
+    res = Result()
+    o = default_options(reverse=reverse, start=start, want_bandwidth=want_bandwidth, **opt_kw)
+    st = ctypes.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+    rc = _lib.lib().pbrcm_reorder_device_noalloc(ctypes.c_void_p(row_ptr_t.data_ptr()),
+                                                 ctypes.c_void_p(col_idx_t.data_ptr()), n, col_idx_t.numel(),
+                                                 ctypes.byref(o), ctypes.c_void_p(perm_t.data_ptr()),
+                                                 ctypes.byref(res), st)
+    if raise_on_error:
+        _check(rc, "pbrcm_reorder_device_noalloc")
+    d = res.as_dict()
+    d["rc"] = rc
+    return d
 
 
 def find_peripheral(row_ptr, col_idx, ctx: Context | None = None):
