@@ -437,10 +437,36 @@ struct Chunk {
         return m > 0 ? (uint32_t)m : (p < pend ? 1u : 0u);
     }
 
+    // Makes the ranked children of the previous chunk (still in shared memory,
+    // with their adjacency in s.pre) the parents of this one: no global load.
+    // Needs Q <= B and Qdeg <= EMAX; K0prev is the edge base they were placed
+    // with.
+    __device__ void form_from_children(uint32_t K0prev)
+    {
+        const uint32_t t = threadIdx.x;
+        const uint32_t F = s.Q, E = s.Qdeg;
+        if (t < F) {
+            const uint32_t x = s.so_idx[t];
+            s.pn[t] = s.ch_node[x];
+            s.prs[t] = s.ch_rs[x];
+            s.pdeg[t] = s.ch_deg[x];
+            s.peb[t] = K0prev + s.so_eoff[t];
+            s.soff[t] = s.so_eoff[t];
+        }
+        s.cc[t] = 0;
+        if (t == 0) {
+            s.soff[F] = E;
+            s.m = F;
+            s.Ec = E;
+            s.hub = 0;
+        }
+        __syncthreads();
+    }
+
     // Finds the child edges of the chunk, compacts them, ranks every
     // parent's children (sorted = by valence, stable; else slot order) and
     // computes the edge offsets of the ranked children.
-    __device__ Agg collect(bool sorted)
+    __device__ Agg collect(bool sorted, bool from_pre = false)
     {
         const uint32_t t = threadIdx.x;
         const uint32_t m = s.m, Ec = s.Ec;
@@ -472,7 +498,9 @@ struct Chunk {
                 jj[r] = j;
                 kk[r] = k;
                 key[r] = base - 1u - (s.peb[j] + k);
-                if (PB_CHECK(M.res, idx < M.nnz, 102))
+                if (from_pre)
+                    c[r] = s.pre[e];  // the parents' adjacency, loaded when they were placed
+                else if (PB_CHECK(M.res, idx < M.nnz, 102))
                     c[r] = ld_ro(M.ci + idx);
             }
         }
@@ -960,26 +988,48 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsi
         if (solo) {
             // ---- CTA 0 alone: chunk by chunk with running offsets ----------
             if (R == 0) {
+                // carry: the frontier and its adjacency are still in shared
+                // memory from the previous level (it fitted one chunk)
+                bool carry = false;
                 while (true) {
                     uint32_t P = st.b, K = st.Kb;
-                    uint32_t p = st.a;
-                    while (p < st.b) {
-                        const uint32_t used = ch.form(p, st.b);
-                        if (s.hub) {
-                            const uint32_t r0 = s.peb[0] - st.Ka;
-                            const Agg g = ch.hub_collect(r0, sorted);
-                            ch.hub_place_and_claim(r0, g.cnt, P, K, write_perm, reverse);
-                            P += g.cnt;
-                            K += g.esum;
-                        } else {
-                            const Agg g = ch.collect(sorted);
-                            ch.place_and_claim(P, K, write_perm, reverse);
-                            P += g.cnt;
-                            K += g.esum;
-                        }
+                    bool next_carry = false;
+                    if (carry) {
+                        ch.form_from_children(st.Ka);
+                        const Agg g = ch.collect(sorted, true);
+                        ch.prefetch();
+                        ch.place_and_claim(P, K, write_perm, reverse);
+                        P += g.cnt;
+                        K += g.esum;
+                        next_carry = g.cnt > 0 && g.cnt <= (uint32_t)B && g.esum <= (uint32_t)EMAX &&
+                                     s.npre == g.esum;
                         __syncthreads();
-                        p += used;
+                    } else {
+                        uint32_t p = st.a;
+                        while (p < st.b) {
+                            const uint32_t used = ch.form(p, st.b);
+                            const bool single = p == st.a && used == st.b - st.a;
+                            if (s.hub) {
+                                const uint32_t r0 = s.peb[0] - st.Ka;
+                                const Agg g = ch.hub_collect(r0, sorted);
+                                ch.hub_place_and_claim(r0, g.cnt, P, K, write_perm, reverse);
+                                P += g.cnt;
+                                K += g.esum;
+                            } else {
+                                const Agg g = ch.collect(sorted);
+                                if (single)
+                                    ch.prefetch();
+                                ch.place_and_claim(P, K, write_perm, reverse);
+                                P += g.cnt;
+                                K += g.esum;
+                                next_carry = single && g.cnt > 0 && g.cnt <= (uint32_t)B &&
+                                             g.esum <= (uint32_t)EMAX && s.npre == g.esum;
+                            }
+                            __syncthreads();
+                            p += used;
+                        }
                     }
+                    carry = next_carry;
                     if (!team.block_ok())
                         return false;
                     const uint32_t tot = P - st.b;

@@ -2,8 +2,9 @@
 //
 // submit() copies a request's CSR into pinned staging and queues it.  A
 // worker thread admits queued requests in arrival order whenever the device
-// bytes in flight stay under the cap and a slot is free, and launches each one
-// at once on the next of S streams: stream-ordered device allocation, H2D,
+// bytes in flight stay under the cap, the CTAs they hold fit the GPU and a
+// stream is free, and launches each one at once on that stream (no request
+// waits behind another in a stream): stream-ordered device allocation, H2D,
 // validation, the reorder kernel (one CTA for small matrices, a cooperative
 // team for large ones or ones with hub rows), D2H of the permutation and the
 // result, an event.  Requests that arrive while others run are launched
@@ -15,6 +16,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -90,6 +92,7 @@ struct Request {
     size_t d_rp = 0, d_ci = 0, d_node = 0, d_rec = 0, d_perm = 0, d_res = 0, d_gs = 0, d_cnt = 0, d_agg = 0,
            d_hub = 0;
     bool team = false;
+    int ctas = 1;       // CTAs of its launch (team size, or 1)
     int stream = 0;
     cudaEvent_t ev = nullptr;
     int state = 0;  // 0 queued, 1 running, 2 done
@@ -104,10 +107,15 @@ struct pbrcm_session {
     uint64_t cap_bytes = 0;
     uint32_t max_inflight = 0;
     std::vector<cudaStream_t> streams;
-    uint32_t next_stream = 0;
+    std::vector<int> stream_busy;  // requests in flight per stream
     int small_variant = 1;
     uint32_t team_cutoff_n = 1u << 18;
-    int team_ctas = 0;
+    int max_ctas = 0;              // largest team (co-resident CTAs of the team kernel)
+    int cap_ctas = 0;              // CTAs the running requests may hold together
+    int ctas_in_use = 0;
+    int team_min = 4, team_max = 64;
+    int idle_team = 0;             // team of a large request that finds the GPU idle (0 = no boost)
+    uint64_t team_nnz = 1ull << 19;
 
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -128,6 +136,7 @@ struct pbrcm_session {
     void run();
     bool launch(Request* r);
     void retire(Request* r);
+    int choose_ctas(const Request* r) const;
 };
 
 namespace {
@@ -197,14 +206,14 @@ bool pbrcm_session::launch(Request* r)
     ok = ok && cudaMemsetAsync(D + r->d_res, 0, sizeof(DevResult), st) == cudaSuccess;
     ok = ok && cudaMemsetAsync(D + r->d_gs, 0, sizeof(GridSync), st) == cudaSuccess;
     if (r->team)
-        ok = ok && cudaMemsetAsync(D + r->d_agg, 0, team_words_bytes(team_ctas), st) == cudaSuccess;
+        ok = ok && cudaMemsetAsync(D + r->d_agg, 0, team_words_bytes(r->ctas), st) == cudaSuccess;
     ok = ok && cudaMemsetAsync(d_counter, 0, 16, st) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(d_job, r->host + r->off_view, sizeof(BatchJob) + sizeof(BatchSlot),
                                cudaMemcpyHostToDevice, st) == cudaSuccess;
     ok = ok && launch_validate(M.rp, M.ci, M.n, M.nnz, M.res, c.sms, st) == cudaSuccess;
     if (r->team)
         ok = ok && launch_team(c.team_variant, M, r->opt, reinterpret_cast<GridSync*>(D + r->d_gs),
-                               reinterpret_cast<unsigned long long*>(D + r->d_agg), team_ctas, st) == cudaSuccess;
+                               reinterpret_cast<unsigned long long*>(D + r->d_agg), r->ctas, st) == cudaSuccess;
     else
         ok = ok && launch_batch(small_variant, d_job, d_slot, 1, d_counter, r->opt, 1, false, st) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(r->host + r->off_perm, M.perm, 4 * (size_t)r->n, cudaMemcpyDeviceToHost, st) ==
@@ -224,9 +233,26 @@ void pbrcm_session::retire(Request* r)
     r->state = 2;
     r->t_done = Clock::now();
     bytes_in_flight -= r->dev_bytes;
+    ctas_in_use -= r->ctas;
+    stream_busy[r->stream] -= 1;
     ++completed;
     lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
     t_last = r->t_done;
+}
+
+// CTAs of a request: 1 for a small matrix; for a large one a team that grows
+// with its nnz (team_min..team_max) -- small teams spend far fewer CTA-seconds
+// per BFS level than the whole GPU -- or, if idle_team is set and nothing else
+// is running or waiting, idle_team CTAs for a lower latency.
+int pbrcm_session::choose_ctas(const Request* r) const
+{
+    if (!r->team)
+        return 1;
+    if (idle_team > 0 && running.empty() && queued.size() <= 1)
+        return std::max(1, std::min(std::min(idle_team, max_ctas), cap_ctas));
+    const uint64_t k = (r->nnz + team_nnz - 1) / team_nnz;
+    const int t = (int)std::max<uint64_t>((uint64_t)team_min, std::min<uint64_t>(k, (uint64_t)team_max));
+    return std::max(1, std::min(t, max_ctas));
 }
 
 void pbrcm_session::run()
@@ -246,12 +272,27 @@ void pbrcm_session::run()
                 ++i;
             }
         }
+        // admit in arrival order while memory, CTAs and a free stream allow
         while (!queued.empty() && running.size() < max_inflight) {
             Request* r = queued.front();
             if (bytes_in_flight + r->dev_bytes > cap_bytes && !running.empty())
                 break;
+            const int need = choose_ctas(r);
+            if (ctas_in_use + need > cap_ctas && !running.empty())
+                break;
+            int free_stream = -1;
+            for (size_t k = 0; k < stream_busy.size(); ++k)
+                if (stream_busy[k] == 0) {
+                    free_stream = (int)k;
+                    break;
+                }
+            if (free_stream < 0)
+                break;
             queued.pop_front();
-            r->stream = (int)(next_stream++ % streams.size());
+            r->stream = free_stream;
+            r->ctas = need;
+            stream_busy[free_stream] += 1;
+            ctas_in_use += need;
             bytes_in_flight += r->dev_bytes;
             peak_bytes = std::max(peak_bytes, bytes_in_flight);
             r->state = 1;
@@ -260,6 +301,8 @@ void pbrcm_session::run()
                 r->state = 2;
                 r->t_done = Clock::now();
                 bytes_in_flight -= r->dev_bytes;
+                ctas_in_use -= need;
+                stream_busy[free_stream] -= 1;
                 ++completed;
             } else {
                 running.push_back(r);
@@ -292,7 +335,7 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
     cudaSetDevice(s->C->device);
     s->cap_bytes = cfg && cfg->memory_cap_bytes ? cfg->memory_cap_bytes : 120ull * 1000 * 1000 * 1000;
     s->max_inflight = cfg && cfg->max_inflight ? cfg->max_inflight : 4096;
-    const uint32_t ns = cfg && cfg->streams ? std::min<uint32_t>(cfg->streams, 64) : 8;
+    const uint32_t ns = cfg && cfg->streams ? std::min<uint32_t>(cfg->streams, 128) : 64;
     for (uint32_t i = 0; i < ns; ++i) {
         cudaStream_t st;
         if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -302,8 +345,17 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
         s->streams.push_back(st);
     }
     s->small_variant = s->C->batch_variant;
-    const int maxc = team_max_ctas(s->C->team_variant, s->C->sms);
-    s->team_ctas = std::max(1, std::min(maxc, s->C->sms / 2));
+    s->max_ctas = std::max(1, team_max_ctas(s->C->team_variant, s->C->sms));
+    s->cap_ctas = std::max(1, batch_max_ctas(s->small_variant, s->C->sms));
+    s->stream_busy.assign(s->streams.size(), 0);
+    if (const char* e = std::getenv("PBRCM_SESSION_TEAM_NNZ"))
+        s->team_nnz = std::max<uint64_t>(1, std::strtoull(e, nullptr, 10));
+    if (const char* e = std::getenv("PBRCM_SESSION_TEAM_MIN"))
+        s->team_min = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("PBRCM_SESSION_TEAM_MAX"))
+        s->team_max = std::max(s->team_min, std::atoi(e));
+    if (const char* e = std::getenv("PBRCM_SESSION_IDLE_TEAM"))
+        s->idle_team = std::max(0, std::atoi(e));
     if (cudaDeviceGetDefaultMemPool(&s->pool, s->C->device) != cudaSuccess) {
         delete s;
         return PBRCM_ERR_CUDA;
@@ -363,7 +415,7 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     r->team = n > s->team_cutoff_n || maxdeg > (uint32_t)emax_small;
     size_t offs[10];
     r->dev_bytes = device_bytes(n, nnz, r->team && maxdeg > (uint32_t)kVariants[s->C->team_variant].emax,
-                                s->team_ctas, offs);
+                                r->team ? s->max_ctas : 1, offs);
     r->d_rp = offs[0];
     r->d_ci = offs[1];
     r->d_node = offs[2];

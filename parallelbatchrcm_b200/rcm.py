@@ -264,13 +264,12 @@ class Session:
         o = default_options(reverse=reverse, start=start, want_bandwidth=want_bandwidth, **opt_kw)
         _check(_lib.lib().pbrcm_session_submit(self.handle, _ptr(rp), _ptr(ci), rp.shape[0] - 1, ci.shape[0],
                                                ctypes.byref(o), ctypes.byref(t)), "pbrcm_session_submit")
-        self._n[t.value] = rp.shape[0] - 1
+        self._n[t.value] = np.empty(max(rp.shape[0] - 1, 1), dtype=np.uint32)
         return t.value
 
     def poll(self, ticket: int):
         """None while running; (perm, result dict) once done."""
-        n = self._n[ticket]
-        perm = np.empty(max(n, 1), dtype=np.uint32)
+        perm = self._n[ticket]
         res = Result()
         done = ctypes.c_int32()
         rc = _lib.lib().pbrcm_session_poll(self.handle, ticket, _ptr(perm), ctypes.byref(res), ctypes.byref(done))
@@ -281,7 +280,7 @@ class Session:
         del self._n[ticket]
         d = res.as_dict()
         d["rc"] = rc
-        return perm[:n], d
+        return perm, d
 
     def drain(self) -> None:
         _check(_lib.lib().pbrcm_session_drain(self.handle), "pbrcm_session_drain")

@@ -224,13 +224,13 @@ def run_serve(args, ws, rank, local):
     torch.cuda.set_device(local)
     ctx = P.Context(local)
     # warm-up both paths
-    _serve_session(ctx, mats[:16], [0.0] * 16, 8)
+    _serve_session(ctx, mats[:16], [0.0] * 16, 96)
     for rp, ci in mats[:4]:
         P.reorder(rp, ci, ctx=ctx)
     rows = []
     for rate in rates:
         arr = list(gaps / rate)
-        lat_s, span_s = _serve_session(ctx, mats, arr, 16)
+        lat_s, span_s = _serve_session(ctx, mats, arr, 96)
         lat_p, span_p = _serve_plain(ctx, mats, arr)
         r = {"rate_per_s": rate,
              "session": {"reorders_per_s": count / span_s, "p50_ms": _quantiles(lat_s)[0],
