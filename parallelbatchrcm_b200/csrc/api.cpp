@@ -111,7 +111,7 @@ int32_t Context::init(int dev)
         return PBRCM_ERR_CUDA;
     if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess)
         return PBRCM_ERR_CUDA;
-    if (cudaMalloc(&d_res, sizeof(DevResult)) != cudaSuccess || cudaMalloc(&d_gs, sizeof(GridSync)) != cudaSuccess)
+    if (cudaMalloc(&d_res, sizeof(DevResult)) != cudaSuccess || cudaMalloc(&d_gs, kTeamParts * sizeof(GridSync)) != cudaSuccess)
         return PBRCM_ERR_OOM;
     if (cudaMallocHost(&h_res, sizeof(DevResult)) != cudaSuccess)
         return PBRCM_ERR_OOM;
@@ -133,7 +133,7 @@ int32_t Context::init(int dev)
     batch_variant = env_int("PBRCM_BATCH_VARIANT", 2);
     if (batch_variant < 0 || batch_variant >= kNumVariants)
         batch_variant = 2;
-    if (cudaMalloc(&d_agg, team_words_bytes(maxc)) != cudaSuccess)
+    if (cudaMalloc(&d_agg, kTeamParts * team_part_bytes(maxc)) != cudaSuccess)
         return PBRCM_ERR_OOM;
     return PBRCM_OK;
 }
@@ -144,7 +144,7 @@ Context::~Context()
         cudaSetDevice(device);
     if (stream)
         cudaStreamSynchronize(stream);
-    for (void* p : {(void*)d_rp, (void*)d_ci, (void*)d_node, (void*)d_perm, (void*)d_rec, (void*)d_hub,
+    for (void* p : {(void*)d_rp, (void*)d_ci, (void*)d_node, (void*)d_perm, (void*)d_rec, (void*)d_rec2, (void*)d_hub,
                     (void*)d_res, (void*)d_gs, (void*)d_agg, (void*)d_jobs, (void*)d_slots, (void*)d_counter, (void*)d_bres,
                     (void*)d_arena})
         if (p)
@@ -181,7 +181,8 @@ bool Context::ensure_single(uint32_t n, uint64_t nnz, bool inputs)
 {
     if (inputs && (!grow(d_rp, cap_rp, (size_t)n + 1) || !grow(d_ci, cap_ci, (size_t)nnz)))
         return false;
-    return grow(d_node, cap_node, n) && grow(d_rec, cap_rec, n) && grow(d_perm, cap_perm, n);
+    return grow(d_node, cap_node, n) && grow(d_rec, cap_rec, n) && grow(d_rec2, cap_rec2, n) &&
+           grow(d_perm, cap_perm, n);
 }
 
 bool Context::ensure_hub(uint64_t nnz) { return grow(d_hub, cap_hub, 4 * (size_t)std::max<uint64_t>(nnz, 1)); }
@@ -200,12 +201,13 @@ int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
         M.nnz = (uint32_t)nnz;
         M.node = d_node;
         M.rec = d_rec;
+        M.rec2 = d_rec2;
         M.perm = perm;
         M.hub = with_hub ? d_hub : nullptr;
         M.res = d_res;
         if (cudaMemsetAsync(d_res, 0, sizeof(DevResult), st) != cudaSuccess ||
-            cudaMemsetAsync(d_gs, 0, sizeof(GridSync), st) != cudaSuccess ||
-            cudaMemsetAsync(d_agg, 0, team_words_bytes(team_ctas), st) != cudaSuccess)
+            cudaMemsetAsync(d_gs, 0, kTeamParts * sizeof(GridSync), st) != cudaSuccess ||
+            cudaMemsetAsync(d_agg, 0, kTeamParts * team_part_bytes(team_ctas), st) != cudaSuccess)
             return PBRCM_ERR_CUDA;
         if (launch_validate(rp, ci, n, (uint32_t)nnz, d_res, sms, st) != cudaSuccess)
             return PBRCM_ERR_CUDA;

@@ -36,6 +36,8 @@ struct Context {
     size_t cap_perm = 0;
     PosRec* d_rec = nullptr;
     size_t cap_rec = 0;
+    PosRec* d_rec2 = nullptr;  // queue records of the speculative ordered pass
+    size_t cap_rec2 = 0;
     uint32_t* d_hub = nullptr;
     size_t cap_hub = 0;
     DevResult* d_res = nullptr;

@@ -98,6 +98,15 @@ __device__ __forceinline__ uint32_t ld_ro(const uint32_t* p) { return __ldg(p); 
 
 __device__ __forceinline__ uint4 ld_node(const NodeEntry* p) { return __ldcg(reinterpret_cast<const uint4*>(p)); }
 
+// The claim word a pass uses: NodeEntry::claim (M.cf == 0) or, for the
+// speculative ordered pass that runs beside a start-search pass, the word
+// NodeEntry::inv (M.cf == 3; inv is only used after the last pass).
+__device__ __forceinline__ uint32_t* claim_ptr(const MatrixView& M, uint32_t v)
+{
+    return reinterpret_cast<uint32_t*>(M.node + v) + M.cf;
+}
+__device__ __forceinline__ uint32_t claim_of(const MatrixView& M, const uint4& nd) { return M.cf ? nd.w : nd.x; }
+
 __device__ __forceinline__ void set_status(DevResult* r, uint32_t code, uint32_t where)
 {
     if (atomicCAS(&r->status, 0u, code) == 0u)
@@ -514,7 +523,7 @@ struct Chunk {
         uint32_t nvalid = 0;
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
-            if (c[r] != kUnvisited && c[r] < M.n && nd[r].x == key[r])
+            if (c[r] != kUnvisited && c[r] < M.n && claim_of(M, nd[r]) == key[r])
                 ++nvalid;
             else
                 c[r] = kUnvisited;
@@ -655,14 +664,14 @@ struct Chunk {
             for (uint32_t f = t; f < Qdeg; f += B) {
                 const uint32_t d = s.pre[f];
                 if (PB_CHECK(M.res, d < M.n, 107))
-                    atomicMax(&M.node[d].claim, kb - f);
+                    atomicMax(claim_ptr(M, d), kb - f);
             }
         } else {
             for_child_edges([&](uint32_t f, uint32_t idx) {
                 if (PB_CHECK(M.res, idx < M.nnz, 106)) {
                     const uint32_t d = ld_ro(M.ci + idx);
                     if (PB_CHECK(M.res, d < M.n, 107))
-                        atomicMax(&M.node[d].claim, kb - f);
+                        atomicMax(claim_ptr(M, d), kb - f);
                 }
             });
         }
@@ -703,7 +712,7 @@ struct Chunk {
                     const uint32_t c = ld_ro(M.ci + rs + e);
                     if (PB_CHECK(M.res, c < M.n, 122)) {
                         const uint4 nd = ld_node(M.node + c);
-                        if (nd.x == base - 1u - (eb + e)) {
+                        if (claim_of(M, nd) == base - 1u - (eb + e)) {
                             dg[r] = nd.z;
                             ok[r] = true;
                             ++nv;
@@ -965,7 +974,7 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsi
     // CTA 0 places the start and claims its edges
     if (R == 0) {
         if (t == 0) {
-            atomicMax(&M.node[start].claim, base);
+            atomicMax(claim_ptr(M, start), base);
             __stcg(reinterpret_cast<uint4*>(M.rec), make_uint4(start, rs0, deg0, 0u));
             if (write_perm)
                 M.perm[reverse ? n - 1 : 0] = start;
@@ -973,7 +982,7 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsi
         for (uint32_t k = t; k < deg0; k += B) {
             const uint32_t d = ld_ro(M.ci + rs0 + k);
             if (PB_CHECK(M.res, d < n, 110))
-                atomicMax(&M.node[d].claim, base - 1u - k);
+                atomicMax(claim_ptr(M, d), base - 1u - k);
         }
     }
     auto is_solo = [&](const LevelState& x) {
@@ -1244,56 +1253,161 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
     init_nodes<B>(M, R, G);
     if (!team.sync(1))
         return;
-    // pass keys: pass p owns [p*kspan, p*kspan + nnz + 1]
+    // pass keys: pass p owns [p*kspan, p*kspan + nnz + 1], separately in
+    // each claim word (claim: start-search and final passes; inv: the
+    // speculative ordered passes)
     const uint32_t kspan = M.nnz + 2u;
     const uint32_t pmax = (uint32_t)(0xFFFFFFFFull / kspan) - 1u;
-    uint32_t pass_id = 0;
-    auto reset_claims = [&]() -> bool {
-        for (uint64_t v = (uint64_t)R * B + t; v < n; v += (uint64_t)G * B)
-            M.node[v].claim = 0u;
-        pass_id = 0;
-        return team.sync(7);
-    };
+    uint32_t pass_id = 0, pass_id2 = 0;
 
+    // Speculation.  Once the first start-search pass has run, every later
+    // pass may be the last one (its eccentricity equals the previous one);
+    // the final ordered pass then starts from the same node.  So the team
+    // splits in two halves: one runs the start-search pass from the
+    // candidate, the other runs the ordered pass from it at the same time
+    // (claim word inv, queue records rec2, writing the output).  If the
+    // candidate is confirmed, the ordered pass is already done; if not, its
+    // output is overwritten later.  Pays off when most levels are small
+    // enough for one CTA (each half runs them on its first CTA); a level that
+    // needs the whole team takes a half team about 1.5x as long.  Not with
+    // hubs (both halves would share the hub scratch).
+    const bool spec = M.rec2 != nullptr && G >= 2 && start == kUnvisited && n > 1 && opt.mode == kModeFull &&
+                      __ldcg(&M.res->maxdeg) <= (uint32_t)EMAX;
+    const uint32_t half = G / 2;
+    const bool low = R < half;
+    const size_t pw = team_part_bytes((int)G) / sizeof(unsigned long long);
+    Team sub = team;  // this CTA's half
+    unsigned long long* sub_agg = agg + (low ? pw : 2 * pw);
+    uint32_t sub_step = 0;
+    if (spec) {
+        sub.size = low ? half : G - half;
+        sub.rank = low ? R : R - half;
+        sub.gs = sub.size > 1 ? team.gs + (low ? 1 : 2) : nullptr;
+        sub.flags = reinterpret_cast<unsigned int*>(sub_agg + 2 * sub.size);
+        sub.expected = sub.size;
+        sub.target = 0;
+        sub.epoch = 0;
+    }
+    MatrixView M2 = M;  // the speculative ordered pass's view
+    M2.rec = M.rec2;
+    M2.cf = 3;
+    bool spec_on = false;    // speculation chosen after the first pass
+    bool spec_done = false;  // the speculative ordered pass wrote the output
+
+    // pseudo-peripheral search (simple_peripheral.cpp:92-141), then the
+    // degree-sorted pass that writes the permutation.  Every pass goes
+    // through the one call of bfs_pass below (it is large: a single inlined
+    // copy keeps the kernel's registers down).
+    bool searching = start == kUnvisited && n > 1;
     if (n == 1) {
         // one node: the start search runs one pass and records nothing
         passes = start == kUnvisited ? 1 : 0;
         start = 0;
-    } else if (start == kUnvisited) {
-        // pseudo-peripheral search (simple_peripheral.cpp:92-141)
+    } else if (searching) {
         start = n / 2;
-        uint32_t lastdist = 0;
-        while (true) {
+    }
+    uint32_t lastdist = 0;
+    while (true) {
+        if (!searching && opt.mode == kModeStartOnly)
+            break;
+        const bool split = searching && spec_on;  // spec_on implies a first pass has run
+        const bool spec_half = split && !low;     // this CTA runs the speculative ordered pass
+        const bool ordered = !searching || spec_half;
+        Team& tm = split ? sub : team;
+        unsigned long long* ag = split ? sub_agg : agg;
+        uint32_t& stp = split ? sub_step : step;
+        uint32_t& pid = spec_half ? pass_id2 : pass_id;
+        if (searching)
             ++passes;
-            if (pass_id + 1 > pmax && !reset_claims())
+        if (pid + 1 > pmax) {
+            // reset this pass's claim word (the other half never touches it)
+            const uint32_t cf = spec_half ? 3u : 0u;
+            for (uint64_t v = (uint64_t)tm.rank * B + t; v < n; v += (uint64_t)tm.size * B)
+                reinterpret_cast<uint32_t*>(M.node + v)[cf] = 0u;
+            pid = 0;
+            if (!tm.sync(7))
                 return;
-            ++pass_id;
-            const uint32_t base = pass_id * kspan + M.nnz + 1u;
-            if (!bfs_pass<B, EMAX>(s, M, team, agg, step, opt, start, base, false, false, false, placed, nlevels,
-                                   last_start))
-                return;
-            if (placed != n) {
+        }
+        ++pid;
+        const uint32_t base = pid * kspan + M.nnz + 1u;
+        const uint32_t step0 = step;
+        uint32_t pl = 0, nl = 0, ls = 0;
+        if (!bfs_pass<B, EMAX>(s, spec_half ? M2 : M, tm, ag, stp, opt, start, base, ordered, ordered,
+                               ordered && opt.reverse != 0, pl, nl, ls))
+            return;
+        if (!searching) {
+            placed = pl;
+            nlevels = nl;
+            last_start = ls;
+            break;
+        }
+        uint32_t dist, next = 0;
+        if (!split) {
+            if (pl != n) {
                 if (R == 0 && t == 0)
                     set_status(M.res, kErrDisconnected, 0);
                 return;
             }
-            const uint32_t dist = nlevels - 1;
+            // speculate only if at most a quarter of the levels needed the
+            // whole team (step counts them)
+            if (passes == 1)
+                spec_on = spec && 4ull * (step - step0) <= nl;
+            dist = nl - 1;
             if (dist == lastdist) {
                 ecc = dist;
-                break;
-            }
-            if (passes > n) {  // eccentricities only grow; cannot happen on a valid run
-                if (R == 0 && t == 0)
-                    set_status(M.res, kErrCheck, 3);
-                return;
+                searching = false;  // the ordered pass from the same start comes next
+                continue;
             }
             if (t == 0)
-                s.bcast[0] = next_peripheral_start(M, opt.outnodes, last_start);
+                s.bcast[0] = next_peripheral_start(M, opt.outnodes, ls);
             __syncthreads();
-            start = s.bcast[0];
-            lastdist = dist;
+            next = s.bcast[0];
             __syncthreads();
+        } else {
+            // the halves meet in the team's GridSync words st[8..12]
+            if (sub.rank == 0 && t == 0) {
+                if (low) {
+                    team.gs->st[8] = pl;
+                    team.gs->st[9] = nl;
+                    team.gs->st[10] = pl == n ? next_peripheral_start(M, opt.outnodes, ls) : 0u;
+                } else {
+                    team.gs->st[11] = pl;
+                    team.gs->st[12] = nl;
+                }
+            }
+            if (!team.sync(10))
+                return;
+            const uint32_t pl_u = __ldcg(&team.gs->st[8]), nl_u = __ldcg(&team.gs->st[9]);
+            next = __ldcg(&team.gs->st[10]);
+            const uint32_t pl_s = __ldcg(&team.gs->st[11]), nl_s = __ldcg(&team.gs->st[12]);
+            if (!team.sync(11))  // everyone has read st[8..12] before the next round writes them
+                return;
+            if (pl_u != n) {
+                if (R == 0 && t == 0)
+                    set_status(M.res, kErrDisconnected, 0);
+                return;
+            }
+            if (pl_s != n || nl_s != nl_u) {  // same start, same levels: cannot differ
+                if (R == 0 && t == 0)
+                    set_status(M.res, kErrCheck, 4);
+                return;
+            }
+            dist = nl_u - 1;
+            if (dist == lastdist) {
+                ecc = dist;
+                placed = pl_s;
+                nlevels = nl_s;
+                spec_done = true;
+                break;
+            }
         }
+        if (passes > n) {  // eccentricities only grow; cannot happen on a valid run
+            if (R == 0 && t == 0)
+                set_status(M.res, kErrCheck, 3);
+            return;
+        }
+        start = next;
+        lastdist = dist;
     }
     if (opt.mode == kModeStartOnly) {
         if (R == 0 && t == 0) {
@@ -1304,14 +1418,6 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
         }
         return;
     }
-    // the final, degree-sorted pass writes the permutation
-    if (pass_id + 1 > pmax && !reset_claims())
-        return;
-    ++pass_id;
-    const uint32_t base = pass_id * kspan + M.nnz + 1u;
-    if (!bfs_pass<B, EMAX>(s, M, team, agg, step, opt, start, base, true, true, opt.reverse != 0, placed, nlevels,
-                           last_start))
-        return;
     if (placed != n) {
         if (R == 0 && t == 0) {
             set_status(M.res, kErrDisconnected, 1);
@@ -1319,11 +1425,12 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
         }
         return;
     }
+    const PosRec* final_rec = spec_done ? M.rec2 : M.rec;
 
     if (opt.want_bw) {
         // inverse permutation (CM positions) into node[].inv
         for (uint64_t pos = (uint64_t)R * B + t; pos < n; pos += (uint64_t)G * B) {
-            const uint4 r = __ldcg(reinterpret_cast<const uint4*>(M.rec) + pos);
+            const uint4 r = __ldcg(reinterpret_cast<const uint4*>(final_rec) + pos);
             M.node[r.x].inv = (uint32_t)pos;
         }
         if (!team.sync(6))

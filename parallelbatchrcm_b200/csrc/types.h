@@ -4,6 +4,12 @@
 #include <cstddef>
 #include <cstdint>
 
+#if defined(__CUDACC__)
+#define PBRCM_HD __host__ __device__
+#else
+#define PBRCM_HD
+#endif
+
 namespace pbrcm {
 
 constexpr uint32_t kUnvisited = 0xFFFFFFFFu;
@@ -74,6 +80,8 @@ struct MatrixView {
     uint32_t* perm;                    // n   output
     uint32_t* hub;                     // 4 * nnz hub scratch, or nullptr if no hub can occur
     DevResult* res;
+    PosRec* rec2;                      // n: queue records of the speculative ordered pass, or nullptr
+    uint32_t cf;                       // claim word of NodeEntry this pass uses (0 claim, 3 inv)
 };
 
 constexpr uint64_t kMaxNnz = 0xFFFFFFF0ull;
@@ -84,6 +92,16 @@ constexpr uint64_t kMaxNnz = 0xFFFFFFF0ull;
 inline size_t team_words_bytes(int ctas)
 {
     return 16 * (size_t)(ctas > 0 ? ctas : 1) + 4 * ((size_t)(ctas > 0 ? ctas : 1) + 8);
+}
+
+// A single-matrix team launch gets kTeamParts sets of team words and
+// GridSyncs: part 0 for the whole team, parts 1 and 2 for its two halves
+// while they run a start-search pass and the speculative ordered pass side
+// by side.  Parts are team_part_bytes apart.
+constexpr int kTeamParts = 3;
+PBRCM_HD inline size_t team_part_bytes(int ctas)
+{
+    return (16 * (size_t)(ctas > 0 ? ctas : 1) + 4 * ((size_t)(ctas > 0 ? ctas : 1) + 8) + 255) & ~(size_t)255;
 }
 
 // One matrix of a batch: its view, its team size (CTAs that reorder it
