@@ -135,6 +135,15 @@ int32_t Context::init(int dev)
         batch_variant = 2;
     if (cudaMalloc(&d_agg, kTeamParts * team_part_bytes(maxc)) != cudaSuccess)
         return PBRCM_ERR_OOM;
+    // cluster teams of the batch path (PBRCM_BATCH_CLUSTER* override)
+    // measured on the mixed 1,024-matrix batch: pairs for the 16 biggest
+    // matrices cut its makespan by ~16 %; larger clusters or more of them
+    // cost more CTA-time than the tail they remove
+    cluster_size = env_int("PBRCM_BATCH_CLUSTER", 2);
+    cluster_nnz = (uint64_t)std::max(1, env_int("PBRCM_BATCH_CLUSTER_NNZ", 1 << 18));
+    cluster_max = env_int("PBRCM_BATCH_CLUSTERS", 16);
+    cluster_solo_parents = (uint32_t)env_int("PBRCM_CLUSTER_SOLO_PARENTS", kVariants[batch_variant].block);
+    cluster_solo_edges = (uint32_t)env_int("PBRCM_CLUSTER_SOLO_EDGES", kVariants[batch_variant].emax);
     return PBRCM_OK;
 }
 

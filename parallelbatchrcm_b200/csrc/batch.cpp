@@ -95,9 +95,26 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
     std::iota(order.begin(), order.end(), 0u);
     std::stable_sort(order.begin(), order.end(),
                      [&](uint32_t a, uint32_t b) { return mats[a].nnz > mats[b].nnz; });
+    // Without CTA teams, the biggest matrices (nnz >= cluster_nnz) go to
+    // thread-block-cluster teams: on one CTA they would set the makespan (a
+    // 200k-node grid takes ~60 ms on one CTA, the whole mixed batch of 1,024
+    // about as long).  The launch is then in clusters: they take the big
+    // matrices first, then their CTAs take the rest one by one.
+    uint32_t nbig = 0;
+    int ncl = 0;
+    if (max_team == 1 && C.cluster_size > 1) {
+        while (nbig < count && mats[order[nbig]].nnz >= C.cluster_nnz)
+            ++nbig;
+        ncl = nbig ? cluster_max_active(v, C.cluster_size) : 0;
+        // one round at most: a team of CTAs spends more CTA-time on a matrix
+        // than one CTA, so only the matrices that would set the tail get one
+        nbig = std::min<uint32_t>(nbig, (uint32_t)std::max(0, C.cluster_max > 0 ? std::min(C.cluster_max, ncl) : ncl));
+        if (ncl <= 0)
+            nbig = 0;
+    }
     std::vector<uint32_t> team(count);
     size_t nslots = 0, teamws = 0;
-    for (uint32_t q = 0; q < count; ++q) {
+    for (uint32_t q = nbig; q < count; ++q) {
         team[q] = team_size(mats[order[q]].nnz, min_nnz, per_cta, max_team);
         nslots += team[q];
         if (team[q] > 1)
@@ -127,7 +144,7 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
     off = team_off + teamws;
     if (!grow_dev(C.d_arena, C.cap_arena, off) || !grow_dev(C.d_jobs, C.cap_jobs, count) ||
         !grow_dev(C.d_bres, C.cap_bres, count) || !grow_dev(C.d_slots, C.cap_slots, nslots) ||
-        !grow_dev(C.d_counter, C.cap_counter, 4))
+        !grow_dev(C.d_counter, C.cap_counter, 8))
         return PBRCM_ERR_OOM;
     unsigned char* A = C.d_arena;
     if (host) {
@@ -158,7 +175,7 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
         J.M.perm = host ? reinterpret_cast<uint32_t*>(A + slot[j].perm) : m.perm_out;
         J.M.hub = nullptr;
         J.M.res = C.d_bres + q;
-        J.team = team[q];
+        J.team = q < nbig ? 1 : team[q];
         if (team[q] > 1) {
             J.gs = reinterpret_cast<GridSync*>(A + tw);
             tw = align128(tw + sizeof(GridSync));
@@ -174,15 +191,24 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
             cudaSuccess ||
         (teamws && cudaMemsetAsync(A + team_off, 0, teamws, st) != cudaSuccess) ||
         cudaMemsetAsync(C.d_bres, 0, sizeof(DevResult) * count, st) != cudaSuccess ||
-        cudaMemsetAsync(C.d_counter, 0, sizeof(uint32_t), st) != cudaSuccess)
+        cudaMemsetAsync(C.d_counter, 0, 2 * sizeof(uint32_t), st) != cudaSuccess)
         return PBRCM_ERR_CUDA;
     if (launch_validate_batch(C.d_jobs, count, C.sms, st) != cudaSuccess)
         return PBRCM_ERR_CUDA;
     cudaEventRecord(C.ev0, st);
-    const int ctas = std::max(1, std::min<int>(maxc, (int)nslots));
-    if (launch_batch(v, C.d_jobs, C.d_slots, (uint32_t)nslots, C.d_counter, opt, ctas, nslots > count, st) !=
-        cudaSuccess)
-        return PBRCM_ERR_CUDA;
+    if (nbig) {
+        Options copt = opt;
+        copt.solo_parents = C.cluster_solo_parents;
+        copt.solo_edges = C.cluster_solo_edges;
+        if (launch_cluster(v, C.d_jobs, nbig, C.d_slots, (uint32_t)nslots, C.d_counter, copt, opt, C.cluster_size,
+                           ncl, st) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+    } else {
+        const int ctas = std::max(1, std::min<int>(maxc, (int)nslots));
+        if (launch_batch(v, C.d_jobs, C.d_slots, (uint32_t)nslots, C.d_counter, opt, ctas, nslots > count, st) !=
+            cudaSuccess)
+            return PBRCM_ERR_CUDA;
+    }
     cudaEventRecord(C.ev1, st);
     std::vector<DevResult> res(count);
     if (cudaMemcpyAsync(res.data(), C.d_bres, sizeof(DevResult) * count, cudaMemcpyDeviceToHost, st) !=

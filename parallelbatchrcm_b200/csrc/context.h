@@ -24,6 +24,11 @@ struct Context {
     uint32_t solo_parents = 0;
     uint32_t barrier = 0;       // team barrier implementation
     int team_maxc = 0;          // co-resident CTAs of the team kernel
+    // batches: the biggest matrices go to thread-block-cluster teams
+    int cluster_size = 2;             // CTAs per cluster (0 or 1: off)
+    uint64_t cluster_nnz = 1u << 18;  // matrices with at least this many entries
+    int cluster_max = 16;             // cap on the matrices given a cluster (0: one per co-resident cluster)
+    uint32_t cluster_solo_parents = 0, cluster_solo_edges = 0;  // solo level bounds inside a cluster
 
     // single-matrix buffers (grow only)
     uint32_t* d_rp = nullptr;

@@ -49,6 +49,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "types.h"
@@ -254,10 +255,20 @@ __device__ __forceinline__ void block_reduce_sum2(unsigned long long& a, unsigne
     __syncthreads();
 }
 
+// Level state of one pass, the same in every CTA of a team.
+struct LevelState {
+    uint32_t a, b;     // frontier positions [a, b)
+    uint32_t Ka, Kb;   // edge ids of the frontier [Ka, Kb)
+    uint32_t L;        // level index of the frontier
+    uint32_t last_start;
+};
+
 // ---------------------------------------------------------------------------
-// Team: one CTA, or all CTAs of a cooperative launch.
+// Team: one CTA, or all CTAs of a cooperative launch (global-memory
+// barriers, all-gather and gate, every wait bounded by wait_ns).
 // ---------------------------------------------------------------------------
 struct Team {
+    static constexpr bool kGrid = true;
     GridSync* gs;        // nullptr for a one-CTA team
     unsigned int* flags; // one barrier flag word per CTA (+ phantom), zeroed per launch
     uint32_t size;       // CTAs in the team
@@ -349,6 +360,289 @@ struct Team {
             return false;
         }
         return true;
+    }
+
+    // Heartbeat of CTA 0's solo run (keeps the gate waiters' bound fresh).
+    __device__ __forceinline__ void beat()
+    {
+        if (gs != nullptr && threadIdx.x == 0)
+            atomicAdd(&gs->heartbeat, 1u);
+    }
+
+    // Bounded wait at the gate for CTA 0 to hand a solo run back.  Thread 0
+    // polls; the wait only runs out if CTA 0's heartbeat stops for wait_ns.
+    __device__ bool gate_wait(LevelState& st)
+    {
+        __shared__ int s_ok;
+        __shared__ uint32_t s_st[6];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int ok = 1;
+            const uint32_t want = epoch + 1;
+            unsigned long long t0 = globaltimer();
+            uint32_t hb = *reinterpret_cast<volatile uint32_t*>(&gs->heartbeat);
+            uint32_t spins = 0;
+            while ((int)(ld_acquire(&gs->epoch) - want) < 0) {
+                if ((++spins & 63u) == 0) {
+                    if (read_status(res) != 0) {
+                        ok = 0;
+                        break;
+                    }
+                    const uint32_t h = *reinterpret_cast<volatile uint32_t*>(&gs->heartbeat);
+                    const unsigned long long now = globaltimer();
+                    if (h != hb) {
+                        hb = h;
+                        t0 = now;
+                    } else if (now - t0 > wait_ns) {
+                        set_status(res, kErrTimeout, 50);
+                        ok = 0;
+                        break;
+                    }
+                }
+                if (spins > 1024)
+                    __nanosleep(256);
+            }
+            if (ok)
+                for (int i = 0; i < 6; ++i)
+                    s_st[i] = __ldcg(&gs->st[i]);
+            s_ok = ok && read_status(res) == 0;
+        }
+        __syncthreads();
+        epoch += 1;
+        if (s_ok) {
+            st.a = s_st[0];
+            st.b = s_st[1];
+            st.Ka = s_st[2];
+            st.Kb = s_st[3];
+            st.L = s_st[4];
+            st.last_start = s_st[5];
+        }
+        return s_ok != 0;
+    }
+
+    // CTA 0 publishes the state and opens the gate.  Returns whether the
+    // team goes on (the waiters read the error status themselves).
+    __device__ bool gate_open(const LevelState& st, bool ok)
+    {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            gs->st[0] = st.a;
+            gs->st[1] = st.b;
+            gs->st[2] = st.Ka;
+            gs->st[3] = st.Kb;
+            gs->st[4] = st.L;
+            gs->st[5] = st.last_start;
+            __threadfence();
+            st_release(&gs->epoch, epoch + 1);
+        }
+        __syncthreads();
+        epoch += 1;
+        return ok;
+    }
+
+    // Level all-gather, first half: this CTA's (children, edges), tagged
+    // with the level's step number.
+    __device__ __forceinline__ void ag_publish(uint32_t cnt, uint32_t esum, uint32_t step, unsigned long long* agg)
+    {
+        if (threadIdx.x == 0) {
+            st_relaxed64(agg + 2 * rank, ((unsigned long long)step << 32) | cnt);
+            st_relaxed64(agg + 2 * rank + 1, ((unsigned long long)step << 32) | esum);
+        }
+    }
+
+    // Second half: the sums over the CTAs before this one (pre) and over
+    // all (all), children in the low and edges in the high 32 bits.
+    template <int B>
+    __device__ bool ag_collect(uint32_t step, const unsigned long long* agg, unsigned long long& pre,
+                               unsigned long long& all, unsigned long long* red)
+    {
+        __shared__ int s_ok;
+        const uint32_t t = threadIdx.x;
+        pre = 0;
+        all = 0;
+        if (t == 0)
+            s_ok = 1;
+        __syncthreads();
+        for (uint32_t i = t; i < size; i += B) {
+            unsigned long long vc, ve;
+            unsigned long long t0 = 0;
+            uint32_t spins = 0;
+            while (true) {
+                vc = ld_relaxed64(agg + 2 * i);
+                ve = ld_relaxed64(agg + 2 * i + 1);
+                if ((uint32_t)(vc >> 32) == step && (uint32_t)(ve >> 32) == step)
+                    break;
+                if ((++spins & 31u) == 0 && !wait_check(t0, 4)) {
+                    s_ok = 0;
+                    break;
+                }
+                if (spins > 2048)
+                    __nanosleep(128);
+            }
+            const unsigned long long v = ((ve & 0xFFFFFFFFull) << 32) | (vc & 0xFFFFFFFFull);
+            all += v;
+            if (i < rank)
+                pre += v;
+        }
+        block_reduce_sum2<B>(pre, all, red);
+        return s_ok != 0;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// ClusterTeam: the CTAs of one thread-block cluster.  The hardware cluster
+// barrier (release / acquire at cluster scope) replaces the global-memory
+// barrier, and the all-gather and the gate hand-over read the peers' shared
+// memory (DSMEM).  A hardware barrier has no time bound, so every CTA of the
+// cluster must reach every barrier: the engine takes each "stop" decision
+// uniformly (from flags all CTAs read after the same barrier) and returns
+// only through such decisions.
+// ---------------------------------------------------------------------------
+struct ClusterShared {
+    unsigned long long ag[2][2];  // all-gather words by barrier phase: children, edges
+    uint32_t ok[2];               // "no error seen" flag at a barrier, by phase
+    uint32_t st[6];               // CTA 0: level state handed over at the gate
+    uint32_t job;                 // CTA 0: the job the cluster works on
+    uint32_t all_ok;              // this CTA's AND of the peers' flags
+};
+
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+
+struct ClusterTeam {
+    static constexpr bool kGrid = false;
+    ClusterShared* cs;  // this CTA's
+    uint32_t size;      // CTAs in the cluster
+    uint32_t rank;      // this CTA's rank in the cluster
+    uint32_t phase;     // cluster barriers passed (slot parity)
+    DevResult* res;
+
+    __device__ __forceinline__ ClusterShared* peer(uint32_t r) const
+    {
+        return cooperative_groups::this_cluster().map_shared_rank(cs, r);
+    }
+
+    __device__ bool block_ok()
+    {
+        __shared__ int s_ok;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_ok = read_status(res) == 0;
+        __syncthreads();
+        return s_ok != 0;
+    }
+
+    // Cluster barrier; true iff no CTA had seen an error when it arrived.
+    __device__ bool sync(uint32_t)
+    {
+        if (size == 1)
+            return block_ok();
+        const uint32_t ph = phase & 1u;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            cs->ok[ph] = read_status(res) == 0 ? 1u : 0u;
+        cluster_arrive();
+        cluster_wait();
+        if (threadIdx.x == 0) {
+            uint32_t a = 1;
+            for (uint32_t r = 0; r < size; ++r)
+                a &= peer(r)->ok[ph];
+            cs->all_ok = a;
+        }
+        __syncthreads();
+        ++phase;
+        return cs->all_ok != 0;
+    }
+
+    __device__ __forceinline__ void beat() {}
+
+    // Every CTA but 0: wait (hardware barrier) for CTA 0 to end its solo run,
+    // then take its level state and its go / stop decision.
+    __device__ bool gate_wait(LevelState& st)
+    {
+        const uint32_t ph = phase & 1u;
+        __syncthreads();
+        cluster_arrive();
+        cluster_wait();
+        if (threadIdx.x == 0) {
+            const ClusterShared* p0 = peer(0);
+            cs->st[0] = p0->st[0];
+            cs->st[1] = p0->st[1];
+            cs->st[2] = p0->st[2];
+            cs->st[3] = p0->st[3];
+            cs->st[4] = p0->st[4];
+            cs->st[5] = p0->st[5];
+            cs->all_ok = p0->ok[ph];
+        }
+        __syncthreads();
+        ++phase;
+        st.a = cs->st[0];
+        st.b = cs->st[1];
+        st.Ka = cs->st[2];
+        st.Kb = cs->st[3];
+        st.L = cs->st[4];
+        st.last_start = cs->st[5];
+        return cs->all_ok != 0;
+    }
+
+    // CTA 0: hand the state over; the decision is CTA 0's alone.
+    __device__ bool gate_open(const LevelState& st, bool ok)
+    {
+        const uint32_t ph = phase & 1u;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            cs->st[0] = st.a;
+            cs->st[1] = st.b;
+            cs->st[2] = st.Ka;
+            cs->st[3] = st.Kb;
+            cs->st[4] = st.L;
+            cs->st[5] = st.last_start;
+            cs->ok[ph] = ok && read_status(res) == 0 ? 1u : 0u;
+        }
+        cluster_arrive();
+        cluster_wait();
+        ++phase;
+        return cs->ok[ph] != 0;
+    }
+
+    // All-gather, first half: publish and arrive (the caller may work before
+    // ag_collect waits).
+    __device__ __forceinline__ void ag_publish(uint32_t cnt, uint32_t esum, uint32_t, unsigned long long*)
+    {
+        const uint32_t ph = phase & 1u;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            cs->ag[ph][0] = cnt;
+            cs->ag[ph][1] = esum;
+            cs->ok[ph] = read_status(res) == 0 ? 1u : 0u;
+        }
+        cluster_arrive();
+    }
+
+    template <int B>
+    __device__ bool ag_collect(uint32_t, const unsigned long long*, unsigned long long& pre, unsigned long long& all,
+                               unsigned long long* red)
+    {
+        const uint32_t ph = phase & 1u;
+        cluster_wait();
+        const uint32_t t = threadIdx.x;
+        pre = 0;
+        all = 0;
+        if (t == 0)
+            cs->all_ok = 1;
+        __syncthreads();
+        for (uint32_t i = t; i < size; i += B) {
+            const ClusterShared* pi = peer(i);
+            const unsigned long long v = (pi->ag[ph][1] << 32) | (pi->ag[ph][0] & 0xFFFFFFFFull);
+            if (!pi->ok[ph])
+                atomicAnd(&cs->all_ok, 0u);
+            all += v;
+            if (i < rank)
+                pre += v;
+        }
+        block_reduce_sum2<B>(pre, all, red);
+        ++phase;
+        return cs->all_ok != 0;
     }
 };
 
@@ -870,90 +1164,14 @@ struct Chunk {
 // ---------------------------------------------------------------------------
 // Level state of one pass.
 // ---------------------------------------------------------------------------
-struct LevelState {
-    uint32_t a, b;     // frontier positions [a, b)
-    uint32_t Ka, Kb;   // edge ids of the frontier [Ka, Kb)
-    uint32_t L;        // level index of the frontier
-    uint32_t last_start;
-};
-
-// Bounded wait at the gate for CTA 0 to hand a solo run back.  Thread 0
-// polls; the wait only runs out if CTA 0's heartbeat stops for wait_ns.
-__device__ __forceinline__ bool gate_wait(Team& team, LevelState& st)
-{
-    __shared__ int s_ok;
-    __shared__ uint32_t s_st[6];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const uint32_t want = team.epoch + 1;
-        unsigned long long t0 = globaltimer();
-        uint32_t hb = *reinterpret_cast<volatile uint32_t*>(&team.gs->heartbeat);
-        uint32_t spins = 0;
-        while ((int)(ld_acquire(&team.gs->epoch) - want) < 0) {
-            if ((++spins & 63u) == 0) {
-                if (read_status(team.res) != 0) {
-                    ok = 0;
-                    break;
-                }
-                const uint32_t h = *reinterpret_cast<volatile uint32_t*>(&team.gs->heartbeat);
-                const unsigned long long now = globaltimer();
-                if (h != hb) {
-                    hb = h;
-                    t0 = now;
-                } else if (now - t0 > team.wait_ns) {
-                    set_status(team.res, kErrTimeout, 50);
-                    ok = 0;
-                    break;
-                }
-            }
-            if (spins > 1024)
-                __nanosleep(256);
-        }
-        if (ok)
-            for (int i = 0; i < 6; ++i)
-                s_st[i] = __ldcg(&team.gs->st[i]);
-        s_ok = ok && read_status(team.res) == 0;
-    }
-    __syncthreads();
-    team.epoch += 1;
-    if (s_ok) {
-        st.a = s_st[0];
-        st.b = s_st[1];
-        st.Ka = s_st[2];
-        st.Kb = s_st[3];
-        st.L = s_st[4];
-        st.last_start = s_st[5];
-    }
-    return s_ok != 0;
-}
-
-// CTA 0 publishes the state and opens the gate.
-__device__ __forceinline__ void gate_open(Team& team, const LevelState& st)
-{
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        team.gs->st[0] = st.a;
-        team.gs->st[1] = st.b;
-        team.gs->st[2] = st.Ka;
-        team.gs->st[3] = st.Kb;
-        team.gs->st[4] = st.L;
-        team.gs->st[5] = st.last_start;
-        __threadfence();
-        st_release(&team.gs->epoch, team.epoch + 1);
-    }
-    __syncthreads();
-    team.epoch += 1;
-}
-
 // ---------------------------------------------------------------------------
 // One ordered BFS pass from `start` with pass key `base`.  Fills
 // rec[0..placed) and, when write_perm, the output.  Returns false if the team
 // must stop.  nlevels: number of levels; last_start: first position of the
 // last level.
 // ---------------------------------------------------------------------------
-template <int B, int EMAX>
-__device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsigned long long* agg,
+template <int B, int EMAX, class TeamT>
+__device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, unsigned long long* agg,
                          uint32_t& step, const Options& opt, uint32_t start, uint32_t base, bool sorted,
                          bool write_perm, bool reverse, uint32_t& placed, uint32_t& nlevels, uint32_t& last_start)
 {
@@ -1000,6 +1218,7 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsi
                 // carry: the frontier and its adjacency are still in shared
                 // memory from the previous level (it fitted one chunk)
                 bool carry = false;
+                bool solo_fail = false;  // stop after handing the gate over
                 while (true) {
                     uint32_t P = st.b, K = st.Kb;
                     bool next_carry = false;
@@ -1039,8 +1258,10 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsi
                         }
                     }
                     carry = next_carry;
-                    if (!team.block_ok())
-                        return false;
+                    if (!team.block_ok()) {
+                        solo_fail = true;
+                        break;
+                    }
                     const uint32_t tot = P - st.b;
                     if (tot == 0) {
                         st.a = st.b;  // an empty frontier marks the end of the pass
@@ -1054,17 +1275,22 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsi
                     st.L += 1;
                     if (st.b > n) {
                         set_status(M.res, kErrCheck, 111);
-                        return false;
+                        solo_fail = true;
+                        break;
                     }
-                    if (G > 1 && t == 0)
-                        atomicAdd(&team.gs->heartbeat, 1u);
+                    if (G > 1)
+                        team.beat();
                     if (!is_solo(st))
                         break;
                 }
-                if (G > 1)
-                    gate_open(team, st);
+                if (G > 1) {
+                    if (!team.gate_open(st, !solo_fail))
+                        return false;
+                } else if (solo_fail) {
+                    return false;
+                }
             } else {
-                if (!gate_wait(team, st))
+                if (!team.gate_wait(st))
                     return false;
             }
             if (st.a == st.b) {
@@ -1102,55 +1328,14 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsi
         }
         // publish (level-tagged), then prefetch while the others finish
         ++step;
-        if (t == 0) {
-            st_relaxed64(agg + 2 * R, ((unsigned long long)step << 32) | my_cnt);
-            st_relaxed64(agg + 2 * R + 1, ((unsigned long long)step << 32) | my_esum);
-        }
+        team.ag_publish(my_cnt, my_esum, step, agg);
         const bool keep = nunits == 1 && !last_hub;
         if (keep)
             ch.prefetch();
         // all-gather of the per-CTA totals
         unsigned long long pre = 0, all = 0;
-        {
-            __shared__ int s_ok;
-            if (t == 0)
-                s_ok = 1;
-            __syncthreads();
-            for (uint32_t i = t; i < G; i += B) {
-                unsigned long long vc, ve;
-                unsigned long long t0 = 0;
-                uint32_t spins = 0;
-                while (true) {
-                    vc = ld_relaxed64(agg + 2 * i);
-                    ve = ld_relaxed64(agg + 2 * i + 1);
-                    if ((uint32_t)(vc >> 32) == step && (uint32_t)(ve >> 32) == step)
-                        break;
-                    if ((++spins & 31u) == 0) {
-                        if (read_status(M.res) != 0) {
-                            s_ok = 0;
-                            break;
-                        }
-                        const unsigned long long now = globaltimer();
-                        if (t0 == 0)
-                            t0 = now;
-                        else if (now - t0 > team.wait_ns) {
-                            set_status(M.res, kErrTimeout, 4);
-                            s_ok = 0;
-                            break;
-                        }
-                    }
-                    if (spins > 2048)
-                        __nanosleep(128);
-                }
-                const unsigned long long v = ((ve & 0xFFFFFFFFull) << 32) | (vc & 0xFFFFFFFFull);
-                all += v;
-                if (i < R)
-                    pre += v;
-            }
-            block_reduce_sum2<B>(pre, all, s.gat64);
-            if (!s_ok)
-                return false;
-        }
+        if (!team.template ag_collect<B>(step, agg, pre, all, s.gat64))
+            return false;
         const uint32_t tot_cnt = (uint32_t)(all & 0xFFFFFFFFull);
         const uint32_t tot_esum = (uint32_t)(all >> 32);
         uint32_t P = st.b + (uint32_t)(pre & 0xFFFFFFFFull);
@@ -1234,8 +1419,8 @@ __device__ void init_nodes(const MatrixView& M, uint32_t R, uint32_t G)
 // Full reorder of one matrix by one team: start search, final ordered pass,
 // bandwidth.  Every CTA of the team runs this; CTA 0 thread 0 writes *res.
 // ---------------------------------------------------------------------------
-template <int B, int EMAX>
-__device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team, unsigned long long* agg,
+template <int B, int EMAX, class TeamT>
+__device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, unsigned long long* agg,
                                const Options& opt)
 {
     const uint32_t t = threadIdx.x;
@@ -1270,23 +1455,26 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
     // output is overwritten later.  Pays off when most levels are small
     // enough for one CTA (each half runs them on its first CTA); a level that
     // needs the whole team takes a half team about 1.5x as long.  Not with
-    // hubs (both halves would share the hub scratch).
-    const bool spec = M.rec2 != nullptr && G >= 2 && start == kUnvisited && n > 1 && opt.mode == kModeFull &&
-                      __ldcg(&M.res->maxdeg) <= (uint32_t)EMAX;
+    // hubs (both halves would share the hub scratch); grid teams only.
+    const bool spec = TeamT::kGrid && M.rec2 != nullptr && G >= 2 && start == kUnvisited && n > 1 &&
+                      opt.mode == kModeFull && __ldcg(&M.res->maxdeg) <= (uint32_t)EMAX;
     const uint32_t half = G / 2;
     const bool low = R < half;
-    const size_t pw = team_part_bytes((int)G) / sizeof(unsigned long long);
-    Team sub = team;  // this CTA's half
-    unsigned long long* sub_agg = agg + (low ? pw : 2 * pw);
+    TeamT sub = team;  // this CTA's half
+    unsigned long long* sub_agg = agg;
     uint32_t sub_step = 0;
-    if (spec) {
-        sub.size = low ? half : G - half;
-        sub.rank = low ? R : R - half;
-        sub.gs = sub.size > 1 ? team.gs + (low ? 1 : 2) : nullptr;
-        sub.flags = reinterpret_cast<unsigned int*>(sub_agg + 2 * sub.size);
-        sub.expected = sub.size;
-        sub.target = 0;
-        sub.epoch = 0;
+    if constexpr (TeamT::kGrid) {
+        if (spec) {
+            const size_t pw = team_part_bytes((int)G) / sizeof(unsigned long long);
+            sub_agg = agg + (low ? pw : 2 * pw);
+            sub.size = low ? half : G - half;
+            sub.rank = low ? R : R - half;
+            sub.gs = sub.size > 1 ? team.gs + (low ? 1 : 2) : nullptr;
+            sub.flags = reinterpret_cast<unsigned int*>(sub_agg + 2 * sub.size);
+            sub.expected = sub.size;
+            sub.target = 0;
+            sub.epoch = 0;
+        }
     }
     MatrixView M2 = M;  // the speculative ordered pass's view
     M2.rec = M.rec2;
@@ -1313,7 +1501,7 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
         const bool split = searching && spec_on;  // spec_on implies a first pass has run
         const bool spec_half = split && !low;     // this CTA runs the speculative ordered pass
         const bool ordered = !searching || spec_half;
-        Team& tm = split ? sub : team;
+        TeamT& tm = split ? sub : team;
         unsigned long long* ag = split ? sub_agg : agg;
         uint32_t& stp = split ? sub_step : step;
         uint32_t& pid = spec_half ? pass_id2 : pass_id;
@@ -1341,7 +1529,7 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
             last_start = ls;
             break;
         }
-        uint32_t dist, next = 0;
+        uint32_t dist = 0, next = 0;
         if (!split) {
             if (pl != n) {
                 if (R == 0 && t == 0)
@@ -1364,41 +1552,43 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, Team& team
             next = s.bcast[0];
             __syncthreads();
         } else {
-            // the halves meet in the team's GridSync words st[8..12]
-            if (sub.rank == 0 && t == 0) {
-                if (low) {
-                    team.gs->st[8] = pl;
-                    team.gs->st[9] = nl;
-                    team.gs->st[10] = pl == n ? next_peripheral_start(M, opt.outnodes, ls) : 0u;
-                } else {
-                    team.gs->st[11] = pl;
-                    team.gs->st[12] = nl;
+            if constexpr (TeamT::kGrid) {
+                // the halves meet in the team's GridSync words st[8..12]
+                if (sub.rank == 0 && t == 0) {
+                    if (low) {
+                        team.gs->st[8] = pl;
+                        team.gs->st[9] = nl;
+                        team.gs->st[10] = pl == n ? next_peripheral_start(M, opt.outnodes, ls) : 0u;
+                    } else {
+                        team.gs->st[11] = pl;
+                        team.gs->st[12] = nl;
+                    }
                 }
-            }
-            if (!team.sync(10))
-                return;
-            const uint32_t pl_u = __ldcg(&team.gs->st[8]), nl_u = __ldcg(&team.gs->st[9]);
-            next = __ldcg(&team.gs->st[10]);
-            const uint32_t pl_s = __ldcg(&team.gs->st[11]), nl_s = __ldcg(&team.gs->st[12]);
-            if (!team.sync(11))  // everyone has read st[8..12] before the next round writes them
-                return;
-            if (pl_u != n) {
-                if (R == 0 && t == 0)
-                    set_status(M.res, kErrDisconnected, 0);
-                return;
-            }
-            if (pl_s != n || nl_s != nl_u) {  // same start, same levels: cannot differ
-                if (R == 0 && t == 0)
-                    set_status(M.res, kErrCheck, 4);
-                return;
-            }
-            dist = nl_u - 1;
-            if (dist == lastdist) {
-                ecc = dist;
-                placed = pl_s;
-                nlevels = nl_s;
-                spec_done = true;
-                break;
+                if (!team.sync(10))
+                    return;
+                const uint32_t pl_u = __ldcg(&team.gs->st[8]), nl_u = __ldcg(&team.gs->st[9]);
+                next = __ldcg(&team.gs->st[10]);
+                const uint32_t pl_s = __ldcg(&team.gs->st[11]), nl_s = __ldcg(&team.gs->st[12]);
+                if (!team.sync(11))  // everyone has read st[8..12] before the next round writes them
+                    return;
+                if (pl_u != n) {
+                    if (R == 0 && t == 0)
+                        set_status(M.res, kErrDisconnected, 0);
+                    return;
+                }
+                if (pl_s != n || nl_s != nl_u) {  // same start, same levels: cannot differ
+                    if (R == 0 && t == 0)
+                        set_status(M.res, kErrCheck, 4);
+                    return;
+                }
+                dist = nl_u - 1;
+                if (dist == lastdist) {
+                    ecc = dist;
+                    placed = pl_s;
+                    nlevels = nl_s;
+                    spec_done = true;
+                    break;
+                }
             }
         }
         if (passes > n) {  // eccentricities only grow; cannot happen on a valid run

@@ -202,6 +202,77 @@ __global__ void __launch_bounds__(256) k_bw_rows(const uint32_t* __restrict__ rp
     }
 }
 
+// A batch launched in thread-block clusters.  First the big matrices,
+// jobs[0..nbig), one per cluster at a time: the cluster's CTA 0 takes the next
+// index from counters[0], the others read it from CTA 0's shared memory, and
+// the cluster reorders the matrix as one ClusterTeam (copt).  Every CTA
+// passes every cluster barrier: the job index and the skip test are the same
+// in all of them, and reorder_matrix stops only through cluster-wide
+// decisions.  When no big matrix is left, every CTA takes the remaining
+// one-CTA slots on its own from counters[1], as k_reorder_batch does.
+template <int B, int EMAX>
+__global__ void __launch_bounds__(B) k_reorder_cluster(const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots,
+                                                       uint32_t nslots, uint32_t* counters, Options copt,
+                                                       Options opt)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto& s = *reinterpret_cast<Smem<B, EMAX>*>(smem_raw);
+    __shared__ ClusterShared cs;
+    __shared__ uint32_t s_job;
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    const uint32_t csize = cl.num_blocks(), crank = cl.block_rank();
+    while (true) {
+        if (crank == 0 && threadIdx.x == 0)
+            cs.job = atomicAdd(counters, 1u);
+        cluster_arrive();
+        cluster_wait();
+        if (threadIdx.x == 0)
+            s_job = cl.map_shared_rank(&cs, 0)->job;
+        __syncthreads();
+        const uint32_t j = s_job;
+        // nobody goes on while a peer still reads its shared memory
+        cluster_arrive();
+        cluster_wait();
+        if (j >= nbig)
+            break;
+        const BatchJob job = jobs[j];
+        if (!skip_matrix<EMAX>(job.M, crank == 0 && threadIdx.x == 0)) {
+            ClusterTeam team{&cs, csize, crank, 0u, job.M.res};
+            reorder_matrix<B, EMAX>(s, job.M, team, nullptr, copt);
+        }
+        cluster_arrive();
+        cluster_wait();
+    }
+    // one-CTA jobs: no cluster barrier and no shared-memory access across CTAs
+    // from here on
+    while (true) {
+        if (threadIdx.x == 0)
+            s.bcast[7] = atomicAdd(counters + 1, 1u);
+        __syncthreads();
+        const uint32_t slot = s.bcast[7];
+        __syncthreads();
+        if (slot >= nslots)
+            break;
+        const BatchSlot sl = slots[slot];
+        const BatchJob job = jobs[sl.job];
+        if (skip_matrix<EMAX>(job.M, threadIdx.x == 0))
+            continue;
+        Team team;
+        team.gs = nullptr;
+        team.flags = nullptr;
+        team.size = 1;
+        team.rank = 0;
+        team.expected = 1;
+        team.mode = 0;
+        team.target = 0;
+        team.epoch = 0;
+        team.wait_ns = opt.wait_ns;
+        team.res = job.M.res;
+        reorder_matrix<B, EMAX>(s, job.M, team, job.words, opt);
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -217,10 +288,57 @@ struct Variant {
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
             if (e != cudaSuccess)
                 return e;
-            return cudaFuncSetAttribute(k_reorder_batch<B, EMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem());
+            e = cudaFuncSetAttribute(k_reorder_batch<B, EMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem());
+            if (e != cudaSuccess)
+                return e;
+            e = cudaFuncSetAttribute(k_reorder_cluster<B, EMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem());
+            if (e != cudaSuccess)
+                return e;
+            return cudaFuncSetAttribute(k_reorder_cluster<B, EMAX>, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                                        1);
         }();
         return once;
+    }
+    static cudaLaunchConfig_t cluster_config(int csize, int nclusters, cudaStream_t st, cudaLaunchAttribute* at)
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(csize * nclusters));
+        cfg.blockDim = dim3(B);
+        cfg.dynamicSmemBytes = smem();
+        cfg.stream = st;
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)csize;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        return cfg;
+    }
+    static int cluster_max_active(int csize)
+    {
+        if (prepare() != cudaSuccess)
+            return 0;
+        cudaLaunchAttribute at[1];
+        cudaLaunchConfig_t cfg = cluster_config(csize, 1, nullptr, at);
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (void*)k_reorder_cluster<B, EMAX>, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        return n;
+    }
+    static cudaError_t cluster(const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots, uint32_t nslots,
+                               uint32_t* counters, const Options& copt, const Options& opt, int csize, int nclusters,
+                               cudaStream_t st)
+    {
+        cudaError_t e = prepare();
+        if (e != cudaSuccess)
+            return e;
+        cudaLaunchAttribute at[1];
+        cudaLaunchConfig_t cfg = cluster_config(csize, nclusters, st, at);
+        return cudaLaunchKernelEx(&cfg, k_reorder_cluster<B, EMAX>, jobs, nbig, slots, nslots, counters, copt, opt);
     }
     static int team_max_ctas(int sms)
     {
@@ -320,6 +438,20 @@ cudaError_t launch_batch(int v, const BatchJob* jobs, const BatchSlot* slots, ui
                          const Options& opt, int ctas, bool cooperative, cudaStream_t st)
 {
     PBRCM_DISPATCH(v, batch(jobs, slots, nslots, counter, opt, ctas, cooperative, st));
+    return cudaErrorInvalidValue;
+}
+
+int cluster_max_active(int v, int csize)
+{
+    PBRCM_DISPATCH(v, cluster_max_active(csize));
+    return 0;
+}
+
+cudaError_t launch_cluster(int v, const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots, uint32_t nslots,
+                           uint32_t* counters, const Options& copt, const Options& opt, int csize, int nclusters,
+                           cudaStream_t st)
+{
+    PBRCM_DISPATCH(v, cluster(jobs, nbig, slots, nslots, counters, copt, opt, csize, nclusters, st));
     return cudaErrorInvalidValue;
 }
 

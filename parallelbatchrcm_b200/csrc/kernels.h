@@ -30,6 +30,13 @@ cudaError_t launch_team(int v, const MatrixView& M, const Options& opt, GridSync
 // cooperative: required when some job has a team of more than one CTA
 cudaError_t launch_batch(int v, const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
                          const Options& opt, int ctas, bool cooperative, cudaStream_t st);
+// A batch in thread-block clusters: jobs[0..nbig) one per cluster (team
+// options copt), then the one-CTA slots by single CTAs (opt); counters[0..1]
+// zeroed per launch.
+int cluster_max_active(int v, int csize);  // co-resident clusters of that size
+cudaError_t launch_cluster(int v, const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots, uint32_t nslots,
+                           uint32_t* counters, const Options& copt, const Options& opt, int csize, int nclusters,
+                           cudaStream_t st);
 cudaError_t launch_bandwidth(const uint32_t* rp, const uint32_t* ci, uint32_t n, const uint32_t* perm, uint32_t* inv,
                              DevResult* res, int sms, cudaStream_t st);
 

@@ -92,6 +92,7 @@ struct Request {
     size_t d_rp = 0, d_ci = 0, d_node = 0, d_rec = 0, d_perm = 0, d_res = 0, d_gs = 0, d_cnt = 0, d_agg = 0,
            d_hub = 0;
     bool team = false;
+    bool cluster = false;  // team as one thread-block cluster (no hub row)
     int ctas = 1;       // CTAs of its launch (team size, or 1)
     int stream = 0;
     cudaEvent_t ev = nullptr;
@@ -115,6 +116,10 @@ struct pbrcm_session {
     int ctas_in_use = 0;
     int team_min = 4, team_max = 64;
     int idle_team = 0;             // team of a large request that finds the GPU idle (0 = no boost)
+    // largest cluster team (0: cooperative teams only).  Off by default: on
+    // the Poisson serving mix, cooperative teams of up to 64 CTAs served
+    // 289 reorders/s against 202-229 for clusters of <= 4-16 CTAs
+    int cluster_max = 0;
     uint64_t team_nnz = 1ull << 19;
 
     std::mutex mu;
@@ -211,7 +216,15 @@ bool pbrcm_session::launch(Request* r)
     ok = ok && cudaMemcpyAsync(d_job, r->host + r->off_view, sizeof(BatchJob) + sizeof(BatchSlot),
                                cudaMemcpyHostToDevice, st) == cudaSuccess;
     ok = ok && launch_validate(M.rp, M.ci, M.n, M.nnz, M.res, c.sms, st) == cudaSuccess;
-    if (r->team)
+    if (r->cluster) {
+        // one thread-block cluster: no cooperative launch, so it runs beside
+        // the other requests' kernels
+        Options copt = r->opt;
+        copt.solo_parents = c.cluster_solo_parents;
+        copt.solo_edges = c.cluster_solo_edges;
+        ok = ok && launch_cluster(small_variant, d_job, 1, d_slot, 0, d_counter, copt, r->opt, r->ctas, 1, st) ==
+                       cudaSuccess;
+    } else if (r->team)
         ok = ok && launch_team(c.team_variant, M, r->opt, reinterpret_cast<GridSync*>(D + r->d_gs),
                                reinterpret_cast<unsigned long long*>(D + r->d_agg), r->ctas, st) == cudaSuccess;
     else
@@ -248,6 +261,15 @@ int pbrcm_session::choose_ctas(const Request* r) const
 {
     if (!r->team)
         return 1;
+    if (r->cluster) {
+        // a power of two up to cluster_max, growing with nnz like a team
+        const uint64_t k = (r->nnz + team_nnz - 1) / team_nnz;
+        const int t = (int)std::max<uint64_t>((uint64_t)team_min, std::min<uint64_t>(k, (uint64_t)cluster_max));
+        int c = 2;
+        while (c * 2 <= t)
+            c *= 2;
+        return c;
+    }
     if (idle_team > 0 && running.empty() && queued.size() <= 1)
         return std::max(1, std::min(std::min(idle_team, max_ctas), cap_ctas));
     const uint64_t k = (r->nnz + team_nnz - 1) / team_nnz;
@@ -356,6 +378,8 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
         s->team_max = std::max(s->team_min, std::atoi(e));
     if (const char* e = std::getenv("PBRCM_SESSION_IDLE_TEAM"))
         s->idle_team = std::max(0, std::atoi(e));
+    if (const char* e = std::getenv("PBRCM_SESSION_CLUSTER_MAX"))
+        s->cluster_max = std::max(0, std::min(16, std::atoi(e)));
     if (cudaDeviceGetDefaultMemPool(&s->pool, s->C->device) != cudaSuccess) {
         delete s;
         return PBRCM_ERR_CUDA;
@@ -413,6 +437,7 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     r->maxdeg = maxdeg;
     const int emax_small = kVariants[s->small_variant].emax;
     r->team = n > s->team_cutoff_n || maxdeg > (uint32_t)emax_small;
+    r->cluster = r->team && s->cluster_max >= 2 && maxdeg <= (uint32_t)emax_small;
     size_t offs[10];
     r->dev_bytes = device_bytes(n, nnz, r->team && maxdeg > (uint32_t)kVariants[s->C->team_variant].emax,
                                 r->team ? s->max_ctas : 1, offs);

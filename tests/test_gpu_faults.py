@@ -88,6 +88,13 @@ def test_bounds_checked_build_agrees(pbrcm):
         "perms, rs = P.reorder_batch(mats, reverse=False, ctx=ctx)\n"
         "for n, p, r in zip(golden_names(), perms, rs):\n"
         "    assert r['status'] == 0 and np.array_equal(p, load_golden(n)['perm']), n\n"
+        "import os\n"
+        "os.environ.update(PBRCM_BATCH_CLUSTER='4', PBRCM_BATCH_CLUSTER_NNZ='1',\n"
+        "                  PBRCM_CLUSTER_SOLO_PARENTS='8', PBRCM_CLUSTER_SOLO_EDGES='32')\n"
+        "ctx2 = P.Context(0)\n"
+        "perms, rs = P.reorder_batch(mats, reverse=False, ctx=ctx2)\n"
+        "for n, p, r in zip(golden_names(), perms, rs):\n"
+        "    assert r['status'] == 0 and np.array_equal(p, load_golden(n)['perm']), ('cluster', n)\n"
         "print('CHECKS_OK')\n"
     ) % (ROOT, os.path.join(ROOT, "tests"))
     env = dict(os.environ, PBRCM_LIB=_lib.CHECKS_LIB)

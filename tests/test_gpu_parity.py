@@ -112,6 +112,42 @@ def test_batch_equals_single(pbrcm, gpu_ctx):
         assert (r["start_node"], r["bandwidth"], r["profile"]) == (s["start_node"], s["bandwidth"], s["profile"])
 
 
+@pytest.mark.parametrize("csize", [2, 8, 16])
+def test_batch_cluster_teams(pbrcm, oracle_mod, csize, monkeypatch):
+    """Every matrix of a batch on thread-block-cluster teams (hardware cluster
+    barriers, all-gather and gate hand-over through distributed shared
+    memory), with small solo bounds so that most levels are split across the
+    cluster's CTAs; a disconnected matrix in the batch reports its error and
+    leaves the others intact."""
+    from parallelbatchrcm_b200 import gen
+    monkeypatch.setenv("PBRCM_BATCH_CLUSTER", str(csize))
+    monkeypatch.setenv("PBRCM_BATCH_CLUSTER_NNZ", "1")
+    monkeypatch.setenv("PBRCM_CLUSTER_SOLO_PARENTS", "8")
+    monkeypatch.setenv("PBRCM_CLUSTER_SOLO_EDGES", "32")
+    ctx = pbrcm.Context(0)
+    try:
+        names = golden_names()
+        mats = [(load_golden(n)["row_ptr"], load_golden(n)["col_idx"]) for n in names]
+        extra = [gen.grid3d(20, 18, 16, seed=31), gen.rgg(20_000, seed=32), gen.grid2d(150, 90, seed=33)]
+        mats += [(m.row_ptr, m.col_idx) for m in extra]
+        a, b = gen.grid2d(12, 9, seed=34), gen.grid2d(5, 4, seed=35)
+        mats.append((np.concatenate([a.row_ptr, b.row_ptr[1:] + a.nnz]).astype(np.uint32),
+                     np.concatenate([a.col_idx, b.col_idx + a.n]).astype(np.uint32)))
+        perms, results = pbrcm.reorder_batch(mats, reverse=False, ctx=ctx, raise_on_error=False)
+        for name, p, r in zip(names, perms, results):
+            g = load_golden(name)
+            assert r["status"] == 0, (name, r)
+            assert np.array_equal(p, g["perm"]), name
+            assert (r["start_node"], r["peripheral_passes"], r["bandwidth"]) == (
+                int(g["start"]), int(g["passes"]), int(g["bandwidth"])), name
+        for m, p, r in zip(extra, perms[len(names):], results[len(names):]):
+            ref = oracle_mod.full_reorder(m.row_ptr, m.col_idx, reverse=False)
+            assert r["status"] == 0 and np.array_equal(p, ref["perm"])
+        assert results[-1]["status"] == 2  # PBRCM_ERR_DISCONNECTED
+    finally:
+        ctx.close()
+
+
 def test_device_entry_point(pbrcm, gpu_ctx):
     import torch
     g = load_golden("rgg_3000_s11")
@@ -123,6 +159,24 @@ def test_device_entry_point(pbrcm, gpu_ctx):
     out = pbrcm.reorder_batch_device([(rp, ci, po)], reverse=False, ctx=gpu_ctx)
     assert out[0]["status"] == 0
     assert np.array_equal(po.cpu().numpy().astype(np.uint32), g["perm"])
+
+
+@pytest.mark.parametrize("cmax", [2, 8])
+def test_session_cluster_teams(pbrcm, gpu_ctx, cmax, monkeypatch):
+    """Requests above the session's one-CTA size run as thread-block-cluster
+    teams (one cluster launch each, next to the other requests' kernels) and
+    give the single-matrix result."""
+    from parallelbatchrcm_b200 import gen
+    monkeypatch.setenv("PBRCM_SESSION_CLUSTER_MAX", str(cmax))
+    mats = [gen.grid3d(68, 68, 68, seed=41), gen.rgg(300_000, seed=42), gen.grid2d(560, 560, seed=43),
+            gen.grid2d(40, 30, seed=44)]
+    with pbrcm.Session(gpu_ctx, streams=8) as sess:
+        tickets = [sess.submit(m.row_ptr, m.col_idx) for m in mats]
+        sess.drain()
+        for m, t in zip(mats, tickets):
+            perm, res = sess.poll(t)
+            q, r = pbrcm.reorder(m.row_ptr, m.col_idx, ctx=gpu_ctx)
+            assert res["status"] == 0 and np.array_equal(perm, q) and res["bandwidth"] == r["bandwidth"]
 
 
 def test_session_results_equal_single(pbrcm, gpu_ctx):
