@@ -695,6 +695,11 @@ struct Chunk {
     Smem<B, EMAX>& s;
     const MatrixView& M;
     uint32_t base;  // key of the pass: edge id e has key base - 1 - e
+    // queue record of position pf_base + threadIdx.x, loaded by the previous
+    // form() for the chunk that follows it (its latency hides behind that
+    // chunk's work); pf_base == kUnvisited: none
+    uint32_t pf_base = kUnvisited;
+    uint4 pf = make_uint4(0u, 0u, 0u, 0u);
 
     // Loads up to B parents starting at position p (< pend) and forms the
     // next chunk: the longest run with <= EMAX edges.  Sets s.m (0 = the
@@ -708,7 +713,7 @@ struct Chunk {
         if (have) {
             const uint32_t pos = p + t;
             if (PB_CHECK(M.res, pos < M.n, 101)) {
-                const uint4 r = __ldcg(reinterpret_cast<const uint4*>(M.rec) + pos);
+                const uint4 r = p == pf_base ? pf : __ldcg(reinterpret_cast<const uint4*>(M.rec) + pos);
                 s.pn[t] = r.x;
                 s.prs[t] = r.y;
                 s.pdeg[t] = r.z;
@@ -733,11 +738,20 @@ struct Chunk {
             if (m == 0)
                 s.soff[0] = 0;
         }
+        // the next chunk starts where this one ends: load its records now
+        const uint32_t used = m > 0 ? (uint32_t)m : (p < pend ? 1u : 0u);
+        const uint32_t nb = p + used;
+        pf_base = kUnvisited;
+        if (nb < pend) {
+            pf_base = nb;
+            if (nb + t < pend && PB_CHECK(M.res, nb + t < M.n, 109))
+                pf = __ldcg(reinterpret_cast<const uint4*>(M.rec) + nb + t);
+        }
         __syncthreads();
         if (t == 0)
             s.Ec = m > 0 ? s.soff[m] : 0;
         __syncthreads();
-        return m > 0 ? (uint32_t)m : (p < pend ? 1u : 0u);
+        return used;
     }
 
     // Makes the ranked children of the previous chunk (still in shared memory,
