@@ -126,9 +126,11 @@ int32_t Context::init(int dev)
     team_ctas = env_int("PBRCM_TEAM_CTAS", 0);
     if (team_ctas <= 0 || team_ctas > maxc)
         team_ctas = std::min(maxc, sms);
-    // levels of at most 2 chunks run on CTA 0 alone
-    solo_parents = (uint32_t)env_int("PBRCM_SOLO_PARENTS", 2 * kVariants[team_variant].block);
-    solo_edges = (uint32_t)env_int("PBRCM_SOLO_EDGES", 2 * kVariants[team_variant].emax);
+    // levels of one chunk run on CTA 0 alone (measured against 2 chunks: the
+    // 128^3 grid 10.55 -> 10.36 ms, a 1000^2 grid 58.9 -> 50.4 ms, a 1M-node
+    // RGG 6.97 -> 6.87 ms; smaller bounds are slower again)
+    solo_parents = (uint32_t)env_int("PBRCM_SOLO_PARENTS", kVariants[team_variant].block);
+    solo_edges = (uint32_t)env_int("PBRCM_SOLO_EDGES", kVariants[team_variant].emax);
     barrier = (uint32_t)env_int("PBRCM_BARRIER", 0) ? 1u : 0u;
     batch_variant = env_int("PBRCM_BATCH_VARIANT", 2);
     if (batch_variant < 0 || batch_variant >= kNumVariants)
