@@ -261,6 +261,42 @@ PBRCM_API int32_t pbrcm_prepare_csr(const uint32_t* row_ptr, const uint32_t* col
 
 PBRCM_API void pbrcm_free(void* p);
 
+/* ---------------------------------------------------------------------- */
+/* Output boundary: the reordered matrix (the reference's `-o`).           */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * B = P A P^T for a permutation perm (perm[k] = original row at position k):
+ * row i of B is row perm[i] of A with every column c renamed to the position
+ * of c, entries sorted by the new column (duplicate entries of A keep their
+ * order).  Replaces CuSolverRCM::reorder (include/device/rcm_cusolver.cuh:
+ * 154-185: cusolverSpXcsrpermHost with p = q = perm, then the values shuffled
+ * through its map).  vals / vals_out: nnz values of val_bytes = 4 or 8 bytes
+ * each, moved with their entries (val_bytes = 0: no values, both may be
+ * NULL).  map_out (nullable, nnz): the entry of A each entry of B came from.
+ * row_ptr_out has n + 1 entries.  A perm that is not a permutation of 0..n-1
+ * returns PBRCM_ERR_ARG.
+ */
+PBRCM_API int32_t pbrcm_permute(pbrcm_context* ctx, const uint32_t* row_ptr, const uint32_t* col_idx,
+                                const void* vals, uint32_t val_bytes, uint32_t n, uint64_t nnz, const uint32_t* perm,
+                                uint32_t* row_ptr_out, uint32_t* col_idx_out, void* vals_out, uint32_t* map_out);
+
+/* The same on device buffers, enqueued on `stream` (a cudaStream_t; NULL =
+ * the context's stream), which is synchronised before returning. */
+PBRCM_API int32_t pbrcm_permute_device(pbrcm_context* ctx, const uint32_t* d_row_ptr, const uint32_t* d_col_idx,
+                                       const void* d_vals, uint32_t val_bytes, uint32_t n, uint64_t nnz,
+                                       const uint32_t* d_perm, uint32_t* d_row_ptr_out, uint32_t* d_col_idx_out,
+                                       void* d_vals_out, uint32_t* d_map_out, void* stream);
+
+/*
+ * Writes a CSR as a MatrixMarket file in the reference's format (storeMTX,
+ * src/COO.cpp:213-251: "coordinate real general", 1-based "row col value"
+ * lines, values printed like std::to_string).  val_bytes 4 = float, 8 =
+ * double; 0 writes "coordinate pattern general" without values.
+ */
+PBRCM_API int32_t pbrcm_store_mtx(const char* path, uint32_t n, uint64_t nnz, const uint32_t* row_ptr,
+                                  const uint32_t* col_idx, const void* vals, uint32_t val_bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -237,3 +237,39 @@ def ref_time(rp, ci, threads: int, steps: int, timeout: float | None = None):
                             str(threads), str(steps)], capture_output=True, text=True, check=True,
                            timeout=timeout)
     return [json.loads(line[5:]) for line in r.stdout.splitlines() if line.startswith("JSON ")]
+
+
+def permute_csr(rp, ci, perm, vals=None):
+    """B = P A P^T as the reference's -o path computes it
+    (include/device/rcm_cusolver.cuh:154-185: cusolverSpXcsrpermHost with
+    p = q = perm, then apply_permutation_in_place of the values through its
+    map): row i of B is row perm[i] of A, columns renamed through the inverse
+    permutation and sorted, equal columns in their original order.  Returns
+    (row_ptr, col_idx, vals or None, map)."""
+    rp, ci, perm = _u32(rp).astype(np.int64), _u32(ci).astype(np.int64), _u32(perm).astype(np.int64)
+    n = rp.shape[0] - 1
+    inv = np.empty(n, np.int64)
+    inv[perm] = np.arange(n)
+    lens = (rp[1:] - rp[:-1])[perm]
+    out_rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=out_rp[1:])
+    row = np.repeat(np.arange(n), lens)
+    idx = rp[perm][row] + (np.arange(out_rp[-1]) - out_rp[row])
+    newc = inv[ci[idx]] if idx.size else np.zeros(0, np.int64)
+    order = np.lexsort((newc, row))  # stable: by row, then new column
+    m = idx[order]
+    return (out_rp.astype(np.uint32), newc[order].astype(np.uint32),
+            (np.asarray(vals)[m] if vals is not None else None), m.astype(np.uint32))
+
+
+def ref_store_mtx(rp, ci, vals, path: str) -> None:
+    """The reference's convert(COO, CSR) + storeMTX (src/CSR.cpp:210-231,
+    src/COO.cpp:213-251) on a CSR with float64 (or float32) values."""
+    with tempfile.TemporaryDirectory() as td:
+        _u32(rp).tofile(os.path.join(td, "rp"))
+        _u32(ci).tofile(os.path.join(td, "ci"))
+        v = np.asarray(vals)
+        v.tofile(os.path.join(td, "v"))
+        mode = "store64" if v.dtype == np.float64 else "store32"
+        subprocess.run([REF_BIN, mode, os.path.join(td, "rp"), os.path.join(td, "ci"), os.path.join(td, "v"), path],
+                       capture_output=True, text=True, check=True)

@@ -14,6 +14,9 @@
 //       loaded CSR to <outprefix>.rp / <outprefix>.ci, then runs `analyze`.
 //   ref_rcm csr <rp> <ci> <outprefix> [start]
 //       Same analysis on a raw CSR taken as is (no prepareRCM).
+//   ref_rcm store64|store32 <rp> <ci> <vals> <out.mtx>
+//       CSR<double|float> with the given values -> convert(COO, CSR)
+//       (CSR.cpp:210-231) -> storeMTX (COO.cpp:213-251).
 //   ref_rcm time <rp> <ci> <threads> <steps>
 //       Times <steps> reorders: findPeripheral + RealCPU::rcm<true> with
 //       <threads> workers (1 = the serial rcm_seq path, else CPU_BATCH with
@@ -149,6 +152,21 @@ int analyze(Graph<float>& g, const std::string& outprefix, long forced_start)
 
 }  // namespace
 
+template <typename T>
+int storeAs(const std::vector<uint32_t>& rp, const std::vector<uint32_t>& ci, std::ifstream& fv, const char* out)
+{
+    const size_t n = rp.size() - 1;
+    CSR<T> csr;
+    csr.alloc(n, n, ci.size());
+    std::memcpy(csr.row_offsets.get(), rp.data(), rp.size() * 4);
+    std::memcpy(csr.col_ids.get(), ci.data(), ci.size() * 4);
+    fv.read(reinterpret_cast<char*>(csr.data.get()), static_cast<std::streamsize>(ci.size() * sizeof(T)));
+    COO<T> coo;
+    convert(coo, csr);
+    storeMTX(coo, out);
+    return 0;
+}
+
 int main(int argc, char** argv)
 {
     try {
@@ -173,6 +191,13 @@ int main(int argc, char** argv)
             Graph<float> g;
             fillGraph(g, readU32(argv[2]), readU32(argv[3]));
             return analyze(g, argv[4], argc >= 6 ? std::atol(argv[5]) : -1);
+        }
+        if (argc >= 6 && (std::strcmp(argv[1], "store64") == 0 || std::strcmp(argv[1], "store32") == 0)) {
+            const std::vector<uint32_t> rp = readU32(argv[2]), ci = readU32(argv[3]);
+            std::ifstream fv(argv[4], std::ios::binary);
+            if (std::strcmp(argv[1], "store64") == 0)
+                return storeAs<double>(rp, ci, fv, argv[5]);
+            return storeAs<float>(rp, ci, fv, argv[5]);
         }
         if (argc >= 6 && std::strcmp(argv[1], "time") == 0) {
             Graph<float> g;

@@ -102,6 +102,9 @@ SIGNATURES = {
     "pbrcm_prepare_csr": (_i32, [_vp, _vp, _u32, _u64, _i32, ctypes.POINTER(ctypes.c_uint64),
                                  ctypes.POINTER(_pu32), ctypes.POINTER(_pu32)]),
     "pbrcm_free": (None, [_vp]),
+    "pbrcm_permute": (_i32, [_vp, _vp, _vp, _vp, _u32, _u32, _u64, _vp, _vp, _vp, _vp, _vp]),
+    "pbrcm_permute_device": (_i32, [_vp, _vp, _vp, _vp, _u32, _u32, _u64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pbrcm_store_mtx": (_i32, [ctypes.c_char_p, _u32, _u64, _vp, _vp, _vp, _u32]),
 }
 
 _lib = None

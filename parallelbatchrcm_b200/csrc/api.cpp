@@ -155,7 +155,7 @@ Context::~Context()
         cudaSetDevice(device);
     if (stream)
         cudaStreamSynchronize(stream);
-    for (void* p : {(void*)d_rp, (void*)d_ci, (void*)d_node, (void*)d_perm, (void*)d_rec, (void*)d_rec2, (void*)d_hub,
+    for (void* p : {(void*)d_pw, (void*)d_rp, (void*)d_ci, (void*)d_node, (void*)d_perm, (void*)d_rec, (void*)d_rec2, (void*)d_hub,
                     (void*)d_res, (void*)d_gs, (void*)d_agg, (void*)d_jobs, (void*)d_slots, (void*)d_counter, (void*)d_bres,
                     (void*)d_arena})
         if (p)
@@ -245,6 +245,52 @@ int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
         break;
     }
     return PBRCM_OK;
+}
+
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// inv (n) | scan partials | long-row list | its counter
+size_t Context::permute_work_bytes(uint32_t n, uint64_t nnz)
+{
+    return al256(4 * (size_t)n) + al256(4 * (size_t)scan_partials_count(n)) +
+           al256(4 * (size_t)permute_long_cap(n, nnz)) + 256;
+}
+
+// B = P A P^T into out_*; validates the CSR first (maxdeg decides whether the
+// long-row scratch is needed) and synchronises `st`.
+int32_t Context::run_permute(const uint32_t* rp, const uint32_t* ci, const void* vals, uint32_t val_bytes, uint32_t n,
+                             uint64_t nnz, const uint32_t* perm, uint32_t* out_rp, uint32_t* out_ci, void* out_vals,
+                             uint32_t* out_map, unsigned char* work, cudaStream_t st)
+{
+    if (cudaMemsetAsync(d_res, 0, sizeof(DevResult), st) != cudaSuccess ||
+        launch_validate(rp, ci, n, (uint32_t)nnz, d_res, sms, st) != cudaSuccess ||
+        cudaMemcpyAsync(h_res, d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return PBRCM_ERR_CUDA;
+    if (h_res->status != kOk)
+        return map_status(h_res->status);
+    uint32_t* scratch = nullptr;
+    uint32_t cap_long = 0;
+    if (h_res->maxdeg > kPermuteWarpRow) {
+        if (!ensure_hub(nnz))
+            return PBRCM_ERR_OOM;
+        scratch = d_hub;
+        cap_long = permute_long_cap(n, nnz);
+    }
+    size_t o = 0;
+    uint32_t* inv = reinterpret_cast<uint32_t*>(work + o);
+    o += al256(4 * (size_t)n);
+    uint32_t* partials = reinterpret_cast<uint32_t*>(work + o);
+    o += al256(4 * (size_t)scan_partials_count(n));
+    uint32_t* longs = reinterpret_cast<uint32_t*>(work + o);
+    o += al256(4 * (size_t)permute_long_cap(n, nnz));
+    uint32_t* nlong = reinterpret_cast<uint32_t*>(work + o);
+    if (launch_permute(rp, ci, vals, val_bytes, n, (uint32_t)nnz, perm, inv, out_rp, out_ci, out_vals, out_map,
+                       partials, longs, cap_long, nlong, scratch, d_res, sms, st) != cudaSuccess ||
+        cudaMemcpyAsync(h_res, d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return PBRCM_ERR_CUDA;
+    return map_status(h_res->status);
 }
 
 static int32_t check_sizes(uint32_t n, uint64_t nnz)
@@ -410,6 +456,67 @@ int32_t pbrcm_reorder_device(pbrcm_context* ctx, const uint32_t* d_row_ptr, cons
             std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     return map_status(r.status);
+}
+
+int32_t pbrcm_permute_device(pbrcm_context* ctx, const uint32_t* d_row_ptr, const uint32_t* d_col_idx,
+                             const void* d_vals, uint32_t val_bytes, uint32_t n, uint64_t nnz, const uint32_t* d_perm,
+                             uint32_t* d_row_ptr_out, uint32_t* d_col_idx_out, void* d_vals_out, uint32_t* d_map_out,
+                             void* stream)
+{
+    if (!d_row_ptr || (!d_col_idx && nnz) || !d_perm || !d_row_ptr_out || (!d_col_idx_out && nnz) ||
+        (val_bytes != 0 && val_bytes != 4 && val_bytes != 8) || (val_bytes && nnz && (!d_vals || !d_vals_out)))
+        return PBRCM_ERR_ARG;
+    if (int32_t rc = check_sizes(n, nnz))
+        return rc;
+    PBRCM_CTX(ctx);
+    Context& C = ctx->ctx;
+    if (!grow(C.d_pw, C.cap_pw, Context::permute_work_bytes(n, nnz)))
+        return PBRCM_ERR_OOM;
+    cudaStream_t st = stream ? (cudaStream_t)stream : C.stream;
+    return C.run_permute(d_row_ptr, d_col_idx, d_vals, val_bytes, n, nnz, d_perm, d_row_ptr_out, d_col_idx_out,
+                         d_vals_out, d_map_out, C.d_pw, st);
+}
+
+int32_t pbrcm_permute(pbrcm_context* ctx, const uint32_t* row_ptr, const uint32_t* col_idx, const void* vals,
+                      uint32_t val_bytes, uint32_t n, uint64_t nnz, const uint32_t* perm, uint32_t* row_ptr_out,
+                      uint32_t* col_idx_out, void* vals_out, uint32_t* map_out)
+{
+    if (!row_ptr || (!col_idx && nnz) || !perm || !row_ptr_out || (!col_idx_out && nnz) ||
+        (val_bytes != 0 && val_bytes != 4 && val_bytes != 8) || (val_bytes && nnz && (!vals || !vals_out)))
+        return PBRCM_ERR_ARG;
+    if (int32_t rc = check_sizes(n, nnz))
+        return rc;
+    PBRCM_CTX(ctx);
+    Context& C = ctx->ctx;
+    const size_t vb = val_bytes ? (size_t)val_bytes * nnz : 0;
+    // work | in: rp, ci, perm, vals | out: rp, ci, vals, map
+    const size_t w = al256(Context::permute_work_bytes(n, nnz));
+    const size_t o_rp = w, o_ci = o_rp + al256(4 * ((size_t)n + 1)), o_pm = o_ci + al256(4 * nnz),
+                 o_v = o_pm + al256(4 * (size_t)n), o_orp = o_v + al256(vb), o_oci = o_orp + al256(4 * ((size_t)n + 1)),
+                 o_ov = o_oci + al256(4 * nnz), o_map = o_ov + al256(vb), total = o_map + al256(4 * nnz);
+    if (!grow(C.d_pw, C.cap_pw, total))
+        return PBRCM_ERR_OOM;
+    unsigned char* D = C.d_pw;
+    cudaStream_t st = C.stream;
+    if (cudaMemcpyAsync(D + o_rp, row_ptr, 4 * ((size_t)n + 1), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        (nnz && cudaMemcpyAsync(D + o_ci, col_idx, 4 * nnz, cudaMemcpyHostToDevice, st) != cudaSuccess) ||
+        cudaMemcpyAsync(D + o_pm, perm, 4 * (size_t)n, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        (vb && cudaMemcpyAsync(D + o_v, vals, vb, cudaMemcpyHostToDevice, st) != cudaSuccess))
+        return PBRCM_ERR_CUDA;
+    int32_t rc = C.run_permute(reinterpret_cast<uint32_t*>(D + o_rp), reinterpret_cast<uint32_t*>(D + o_ci),
+                               vb ? D + o_v : nullptr, val_bytes, n, nnz, reinterpret_cast<uint32_t*>(D + o_pm),
+                               reinterpret_cast<uint32_t*>(D + o_orp), reinterpret_cast<uint32_t*>(D + o_oci),
+                               vb ? D + o_ov : nullptr, map_out ? reinterpret_cast<uint32_t*>(D + o_map) : nullptr, D,
+                               st);
+    if (rc != PBRCM_OK)
+        return rc;
+    if (cudaMemcpyAsync(row_ptr_out, D + o_orp, 4 * ((size_t)n + 1), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        (nnz && cudaMemcpyAsync(col_idx_out, D + o_oci, 4 * nnz, cudaMemcpyDeviceToHost, st) != cudaSuccess) ||
+        (vb && cudaMemcpyAsync(vals_out, D + o_ov, vb, cudaMemcpyDeviceToHost, st) != cudaSuccess) ||
+        (map_out && nnz && cudaMemcpyAsync(map_out, D + o_map, 4 * nnz, cudaMemcpyDeviceToHost, st) != cudaSuccess) ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return PBRCM_ERR_CUDA;
+    return PBRCM_OK;
 }
 
 int32_t pbrcm_find_peripheral(pbrcm_context* ctx, const uint32_t* row_ptr, const uint32_t* col_idx, uint32_t n,

@@ -50,6 +50,10 @@ struct Context {
     GridSync* d_gs = nullptr;
     unsigned long long* d_agg = nullptr;
 
+    // matrix permutation workspace (grow only)
+    unsigned char* d_pw = nullptr;
+    size_t cap_pw = 0;
+
     // batch buffers (grow only)
     BatchJob* d_jobs = nullptr;
     size_t cap_jobs = 0;
@@ -66,6 +70,10 @@ struct Context {
     ~Context();
     bool ensure_single(uint32_t n, uint64_t nnz, bool inputs);
     bool ensure_hub(uint64_t nnz);
+    int32_t run_permute(const uint32_t* rp, const uint32_t* ci, const void* vals, uint32_t val_bytes, uint32_t n,
+                        uint64_t nnz, const uint32_t* perm, uint32_t* out_rp, uint32_t* out_ci, void* out_vals,
+                        uint32_t* out_map, unsigned char* work, cudaStream_t st);
+    static size_t permute_work_bytes(uint32_t n, uint64_t nnz);
     int32_t run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint64_t nnz, uint32_t* perm,
                        const Options& opt, cudaStream_t st, DevResult* out, float* dev_ms);
 };

@@ -475,6 +475,12 @@ cudaError_t launch_validate_batch(const BatchJob* jobs, uint32_t njobs, int sms,
     return cudaGetLastError();
 }
 
+void launch_perm_inverse(const uint32_t* perm, uint32_t n, uint32_t* inv, DevResult* res, int blocks,
+                         cudaStream_t st)
+{
+    k_bw_inverse<<<blocks, 256, 0, st>>>(perm, n, inv, res);
+}
+
 cudaError_t launch_bandwidth(const uint32_t* rp, const uint32_t* ci, uint32_t n, const uint32_t* perm, uint32_t* inv,
                              DevResult* res, int sms, cudaStream_t st)
 {

@@ -37,6 +37,24 @@ int cluster_max_active(int v, int csize);  // co-resident clusters of that size
 cudaError_t launch_cluster(int v, const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots, uint32_t nslots,
                            uint32_t* counters, const Options& copt, const Options& opt, int csize, int nclusters,
                            cudaStream_t st);
+// inv[perm[k]] = k over a zeroed-to-0xFF inv; a non-permutation posts
+// kErrArg (kernels.cu)
+void launch_perm_inverse(const uint32_t* perm, uint32_t n, uint32_t* inv, DevResult* res, int blocks,
+                         cudaStream_t st);
+// B = P A P^T (permute.cu): row_ptr_out (n+1), col_idx_out (nnz), values of
+// val_bytes 0 / 4 / 8 and the source map (nullable) from row_ptr, col_idx,
+// values and perm.  Workspace: inv (n), partials (scan_partials_count(n)),
+// long_rows (cap_long = permute_long_cap(n, nnz)) and its counter, scratch
+// (4 * nnz, only needed when a row has more than 1,024 entries; else nullptr
+// and cap_long 0).
+cudaError_t launch_permute(const uint32_t* rp, const uint32_t* ci, const void* vals, uint32_t val_bytes, uint32_t n,
+                           uint32_t nnz, const uint32_t* perm, uint32_t* inv, uint32_t* out_rp, uint32_t* out_ci,
+                           void* out_vals, uint32_t* out_map, uint32_t* partials, uint32_t* long_rows,
+                           uint32_t cap_long, uint32_t* nlong, uint32_t* scratch, DevResult* res, int sms,
+                           cudaStream_t st);
+uint32_t scan_partials_count(uint32_t n);
+uint32_t permute_long_cap(uint32_t n, uint64_t nnz);
+constexpr uint32_t kPermuteWarpRow = 1024;  // longest row of the warp path
 cudaError_t launch_bandwidth(const uint32_t* rp, const uint32_t* ci, uint32_t n, const uint32_t* perm, uint32_t* inv,
                              DevResult* res, int sms, cudaStream_t st);
 

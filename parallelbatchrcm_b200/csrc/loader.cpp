@@ -348,4 +348,43 @@ int32_t pbrcm_prepare_csr(const uint32_t* row_ptr, const uint32_t* col_idx, uint
 
 void pbrcm_free(void* p) { std::free(p); }
 
+int32_t pbrcm_store_mtx(const char* path, uint32_t n, uint64_t nnz, const uint32_t* row_ptr, const uint32_t* col_idx,
+                        const void* vals, uint32_t val_bytes)
+{
+    if (!path || !row_ptr || (!col_idx && nnz) || (val_bytes != 0 && val_bytes != 4 && val_bytes != 8) ||
+        (val_bytes && nnz && !vals) || row_ptr[n] != nnz)
+        return PBRCM_ERR_ARG;
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f)
+        return PBRCM_ERR_IO;
+    std::string buf;
+    buf.reserve(1 << 22);
+    buf += val_bytes ? "%%MatrixMarket matrix coordinate real general\n"
+                     : "%%MatrixMarket matrix coordinate pattern general\n";
+    buf += std::to_string(n) + " " + std::to_string(n) + " " + std::to_string(nnz) + "\n";
+    bool ok = true;
+    for (uint32_t r = 0; r < n && ok; ++r) {
+        for (uint32_t k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+            buf += std::to_string((unsigned long)r + 1);
+            buf += ' ';
+            buf += std::to_string((unsigned long)col_idx[k] + 1);
+            if (val_bytes == 4) {
+                buf += ' ';
+                buf += std::to_string(static_cast<const float*>(vals)[k]);
+            } else if (val_bytes == 8) {
+                buf += ' ';
+                buf += std::to_string(static_cast<const double*>(vals)[k]);
+            }
+            buf += '\n';
+        }
+        if (buf.size() >= (1u << 22)) {
+            ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+            buf.clear();
+        }
+    }
+    ok = ok && std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? PBRCM_OK : PBRCM_ERR_IO;
+}
+
 }  // extern "C"

@@ -32,7 +32,8 @@ from ._lib import AUTO_START, DEBUG_PHANTOM_CTA, Matrix, Options, Result, Sessio
 __all__ = [
     "PbrcmError", "Context", "default_options", "reorder", "reorder_device", "reorder_device_noalloc",
     "find_peripheral",
-    "bandwidth", "reorder_batch", "reorder_batch_device", "Session", "load_mtx", "prepare_csr",
+    "bandwidth", "reorder_batch", "reorder_batch_device", "Session", "load_mtx", "prepare_csr", "permute",
+    "permute_device", "store_mtx",
     "Graph", "GPU_BATCH", "SimplePeripheral", "compute_bandwidth", "check_bandwidth", "max_valency",
     "check_permutation", "AUTO_START", "DEBUG_PHANTOM_CTA",
 ]
@@ -319,6 +320,63 @@ def load_mtx(path: str):
     _check(_lib.lib().pbrcm_load_mtx(path.encode(), ctypes.byref(n), ctypes.byref(nnz), ctypes.byref(rp_p),
                                      ctypes.byref(ci_p)), f"pbrcm_load_mtx({path})")
     return _take_csr(n.value, nnz.value, rp_p, ci_p)
+
+
+def _vals(vals):
+    if vals is None:
+        return None, 0
+    v = np.ascontiguousarray(vals)
+    if v.dtype.itemsize not in (4, 8):
+        raise ValueError("values must have 4 or 8 bytes per entry")
+    return v, v.dtype.itemsize
+
+
+def permute(row_ptr, col_idx, perm, vals=None, *, want_map: bool = False, ctx: Context | None = None):
+    """B = P A P^T (the reference's `-o` reordering, CuSolverRCM::reorder,
+    include/device/rcm_cusolver.cuh:154-185): row i of B is row perm[i] of A
+    with columns renamed to their positions and sorted.  Returns (row_ptr,
+    col_idx, vals or None, map or None); map[k] = entry of A behind entry k."""
+    rp, ci, pm = _u32(row_ptr), _u32(col_idx), _u32(perm)
+    v, vb = _vals(vals)
+    n, nnz = rp.shape[0] - 1, ci.shape[0]
+    orp = np.empty(n + 1, np.uint32)
+    oci = np.empty(max(nnz, 1), np.uint32)
+    ov = np.empty(max(nnz, 1), v.dtype) if v is not None else None
+    om = np.empty(max(nnz, 1), np.uint32) if want_map else None
+    _check(_lib.lib().pbrcm_permute(_h(ctx), _ptr(rp), _ptr(ci), _ptr(v) if v is not None else None, vb, n, nnz,
+                                    _ptr(pm), _ptr(orp), _ptr(oci), _ptr(ov) if ov is not None else None,
+                                    _ptr(om) if om is not None else None), "pbrcm_permute")
+    return orp, oci[:nnz], (ov[:nnz] if ov is not None else None), (om[:nnz] if om is not None else None)
+
+
+def permute_device(row_ptr_t, col_idx_t, perm_t, vals_t=None, *, want_map: bool = False,
+                   ctx: Context | None = None, stream=None):
+    """permute() on device-resident torch tensors.  Returns (row_ptr, col_idx,
+    vals or None, map or None) as tensors on the same device."""
+    import torch
+
+    n, nnz = row_ptr_t.numel() - 1, col_idx_t.numel()
+    dev = row_ptr_t.device
+    orp = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    oci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+    ov = torch.empty(max(nnz, 1), dtype=vals_t.dtype, device=dev) if vals_t is not None else None
+    om = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev) if want_map else None
+    vb = vals_t.element_size() if vals_t is not None else 0
+    st = stream.cuda_stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    _check(_lib.lib().pbrcm_permute_device(
+        _h(ctx), row_ptr_t.data_ptr(), col_idx_t.data_ptr(), vals_t.data_ptr() if vals_t is not None else None,
+        vb, n, nnz, perm_t.data_ptr(), orp.data_ptr(), oci.data_ptr(), ov.data_ptr() if ov is not None else None,
+        om.data_ptr() if om is not None else None, st), "pbrcm_permute_device")
+    return orp, oci[:nnz], (ov[:nnz] if ov is not None else None), (om[:nnz] if om is not None else None)
+
+
+def store_mtx(path: str, row_ptr, col_idx, vals=None):
+    """Writes a MatrixMarket file in the reference's storeMTX format
+    (src/COO.cpp:213-251); without values a `pattern` file."""
+    rp, ci = _u32(row_ptr), _u32(col_idx)
+    v, vb = _vals(vals)
+    _check(_lib.lib().pbrcm_store_mtx(path.encode(), rp.shape[0] - 1, ci.shape[0], _ptr(rp), _ptr(ci),
+                                      _ptr(v) if v is not None else None, vb), f"pbrcm_store_mtx({path})")
 
 
 def prepare_csr(row_ptr, col_idx, check_symmetry: bool = True):
