@@ -113,7 +113,8 @@ int32_t Context::init(int dev)
         return PBRCM_ERR_CUDA;
     if (cudaMalloc(&d_res, sizeof(DevResult)) != cudaSuccess || cudaMalloc(&d_gs, kTeamParts * sizeof(GridSync)) != cudaSuccess)
         return PBRCM_ERR_OOM;
-    if (cudaMallocHost(&h_res, sizeof(DevResult)) != cudaSuccess)
+    if (cudaMallocHost(&h_res, sizeof(DevResult)) != cudaSuccess ||
+        cudaMallocHost(&h_aux, 64) != cudaSuccess)
         return PBRCM_ERR_OOM;
     // team shape: variant and CTA count (PBRCM_TEAM_VARIANT / PBRCM_TEAM_CTAS override)
     team_variant = env_int("PBRCM_TEAM_VARIANT", 1);
@@ -162,6 +163,8 @@ Context::~Context()
             cudaFree(p);
     if (h_res)
         cudaFreeHost(h_res);
+    if (h_aux)
+        cudaFreeHost(h_aux);
     if (ev0)
         cudaEventDestroy(ev0);
     if (ev1)
@@ -249,47 +252,52 @@ int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
 
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// inv (n) | scan partials | long-row list | its counter
+// inv (n) | scan partials | mid-row list (n) | long-row list | counters
 size_t Context::permute_work_bytes(uint32_t n, uint64_t nnz)
 {
-    return al256(4 * (size_t)n) + al256(4 * (size_t)scan_partials_count(n)) +
+    return 2 * al256(4 * (size_t)n) + al256(4 * (size_t)scan_partials_count(n)) +
            al256(4 * (size_t)permute_long_cap(n, nnz)) + 256;
 }
 
-// B = P A P^T into out_*; validates the CSR first (maxdeg decides whether the
-// long-row scratch is needed) and synchronises `st`.
+// B = P A P^T into out_*, after the CSR check on the same stream (the
+// permutation kernels bound every access themselves, so they need not wait
+// for its verdict); one synchronisation of `st`, two if a row has more than
+// 1,024 entries and the long-row scratch has to be allocated first.
 int32_t Context::run_permute(const uint32_t* rp, const uint32_t* ci, const void* vals, uint32_t val_bytes, uint32_t n,
                              uint64_t nnz, const uint32_t* perm, uint32_t* out_rp, uint32_t* out_ci, void* out_vals,
                              uint32_t* out_map, unsigned char* work, cudaStream_t st)
 {
-    if (cudaMemsetAsync(d_res, 0, sizeof(DevResult), st) != cudaSuccess ||
-        launch_validate(rp, ci, n, (uint32_t)nnz, d_res, sms, st) != cudaSuccess ||
-        cudaMemcpyAsync(h_res, d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-        return PBRCM_ERR_CUDA;
-    if (h_res->status != kOk)
-        return map_status(h_res->status);
-    uint32_t* scratch = nullptr;
-    uint32_t cap_long = 0;
-    if (h_res->maxdeg > kPermuteWarpRow) {
-        if (!ensure_hub(nnz))
-            return PBRCM_ERR_OOM;
-        scratch = d_hub;
-        cap_long = permute_long_cap(n, nnz);
-    }
     size_t o = 0;
     uint32_t* inv = reinterpret_cast<uint32_t*>(work + o);
     o += al256(4 * (size_t)n);
     uint32_t* partials = reinterpret_cast<uint32_t*>(work + o);
     o += al256(4 * (size_t)scan_partials_count(n));
+    uint32_t* mids = reinterpret_cast<uint32_t*>(work + o);
+    o += al256(4 * (size_t)n);
     uint32_t* longs = reinterpret_cast<uint32_t*>(work + o);
     o += al256(4 * (size_t)permute_long_cap(n, nnz));
-    uint32_t* nlong = reinterpret_cast<uint32_t*>(work + o);
-    if (launch_permute(rp, ci, vals, val_bytes, n, (uint32_t)nnz, perm, inv, out_rp, out_ci, out_vals, out_map,
-                       partials, longs, cap_long, nlong, scratch, d_res, sms, st) != cudaSuccess ||
+    uint32_t* counters = reinterpret_cast<uint32_t*>(work + o);
+    const uint32_t cap_long = permute_long_cap(n, nnz);
+    uint32_t* scratch = d_hub != nullptr && cap_hub >= 4 * (size_t)std::max<uint64_t>(nnz, 1) ? d_hub : nullptr;
+    if (cudaMemsetAsync(d_res, 0, sizeof(DevResult), st) != cudaSuccess ||
+        launch_validate(rp, ci, n, (uint32_t)nnz, d_res, sms, st) != cudaSuccess ||
+        launch_permute(rp, ci, vals, val_bytes, n, (uint32_t)nnz, perm, inv, out_rp, out_ci, out_vals, out_map,
+                       partials, mids, longs, cap_long, counters, scratch, d_res, sms, st) != cudaSuccess ||
         cudaMemcpyAsync(h_res, d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(h_aux, counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return PBRCM_ERR_CUDA;
+    if (h_res->status != kOk)
+        return map_status(h_res->status);
+    if (h_aux[1] > 0 && scratch == nullptr) {
+        if (!ensure_hub(nnz))
+            return PBRCM_ERR_OOM;
+        if (launch_permute_long(rp, ci, vals, val_bytes, n, (uint32_t)nnz, perm, inv, out_rp, out_ci, out_vals,
+                                out_map, longs, cap_long, counters, d_hub, d_res, sms, st) != cudaSuccess ||
+            cudaMemcpyAsync(h_res, d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+    }
     return map_status(h_res->status);
 }
 

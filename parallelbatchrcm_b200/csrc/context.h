@@ -47,6 +47,7 @@ struct Context {
     size_t cap_hub = 0;
     DevResult* d_res = nullptr;
     DevResult* h_res = nullptr;
+    uint32_t* h_aux = nullptr;  // pinned words read back with a result
     GridSync* d_gs = nullptr;
     unsigned long long* d_agg = nullptr;
 

@@ -44,14 +44,20 @@ void launch_perm_inverse(const uint32_t* perm, uint32_t n, uint32_t* inv, DevRes
 // B = P A P^T (permute.cu): row_ptr_out (n+1), col_idx_out (nnz), values of
 // val_bytes 0 / 4 / 8 and the source map (nullable) from row_ptr, col_idx,
 // values and perm.  Workspace: inv (n), partials (scan_partials_count(n)),
-// long_rows (cap_long = permute_long_cap(n, nnz)) and its counter, scratch
-// (4 * nnz, only needed when a row has more than 1,024 entries; else nullptr
-// and cap_long 0).
+// mid_rows (n), long_rows (cap_long = permute_long_cap(n, nnz)), counters
+// (2), scratch (4 * nnz, only needed when a row has more than 1,024
+// entries; else nullptr and cap_long 0).
 cudaError_t launch_permute(const uint32_t* rp, const uint32_t* ci, const void* vals, uint32_t val_bytes, uint32_t n,
                            uint32_t nnz, const uint32_t* perm, uint32_t* inv, uint32_t* out_rp, uint32_t* out_ci,
-                           void* out_vals, uint32_t* out_map, uint32_t* partials, uint32_t* long_rows,
-                           uint32_t cap_long, uint32_t* nlong, uint32_t* scratch, DevResult* res, int sms,
-                           cudaStream_t st);
+                           void* out_vals, uint32_t* out_map, uint32_t* partials, uint32_t* mid_rows,
+                           uint32_t* long_rows, uint32_t cap_long, uint32_t* counters, uint32_t* scratch,
+                           DevResult* res, int sms, cudaStream_t st);
+// the long rows launch_permute listed (counters[1]) when it had no scratch
+cudaError_t launch_permute_long(const uint32_t* rp, const uint32_t* ci, const void* vals, uint32_t val_bytes,
+                                uint32_t n, uint32_t nnz, const uint32_t* perm, const uint32_t* inv,
+                                const uint32_t* out_rp, uint32_t* out_ci, void* out_vals, uint32_t* out_map,
+                                const uint32_t* long_rows, uint32_t cap_long, const uint32_t* counters,
+                                uint32_t* scratch, DevResult* res, int sms, cudaStream_t st);
 uint32_t scan_partials_count(uint32_t n);
 uint32_t permute_long_cap(uint32_t n, uint64_t nnz);
 constexpr uint32_t kPermuteWarpRow = 1024;  // longest row of the warp path

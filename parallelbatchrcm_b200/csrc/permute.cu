@@ -10,10 +10,12 @@
 // scatter:
 //   1. inv[perm[k]] = k with a bijection check (k_bw_inverse, kernels.cu);
 //   2. new row lengths, scanned into row_ptr_out (three small kernels);
-//   3. one warp per row of at most kWarpRow entries: the renamed columns go to
-//      the warp's shared memory and every entry's rank is counted there
-//      (rows of sparse matrices are short: 5-27 entries for grids);
-//   4. one CTA per longer row: a stable 8-bit LSD radix sort of (new column,
+//   3. eight lanes per row of at most kGroupRow entries (rows of sparse
+//      matrices are short: 5-7 for grids), four rows per warp: the row's
+//      entries load coalesced and are ranked with shuffles;
+//   4. one warp per listed row of at most kWarpRow entries: the same rank
+//      count over the warp's shared memory;
+//   5. one CTA per longer row: a stable 8-bit LSD radix sort of (new column,
 //      slot) in global scratch (4 words per entry).
 #include <algorithm>
 #include <cstdint>
@@ -27,6 +29,7 @@ namespace pbrcm {
 
 namespace {
 
+constexpr uint32_t kGroupRow = 8;               // longest row the lane-group path takes
 constexpr int kWarpRow = (int)kPermuteWarpRow;  // longest row the warp path takes
 constexpr int kRowWarps = 8;       // warps per CTA of the warp path
 constexpr int kScanItems = 8;      // elements per thread of the scan
@@ -157,27 +160,83 @@ struct PermView {
     DevResult* res;
 };
 
-// Row i of B by one warp (rows of at most kWarpRow entries); longer rows are
-// listed for k_permute_long.
+// Rows of B of at most kGroupRow entries, kGroupRow lanes each (four rows
+// per warp): a row's entries load with adjacent lanes (coalesced), the
+// renamed columns are ranked across the group with shuffles.  Longer rows are
+// listed for k_permute_rows (mid[0..counters[0])).
 template <typename V>
-__global__ void __launch_bounds__(kRowWarps * 32) k_permute_rows(PermView a, uint32_t* long_rows, uint32_t cap_long,
-                                                                 uint32_t* nlong)
+__global__ void __launch_bounds__(256) k_permute_short(PermView a, uint32_t* mid, uint32_t* counters)
+{
+    constexpr uint32_t G = kGroupRow;
+    const V* vals = static_cast<const V*>(a.vals);
+    V* out_vals = static_cast<V*>(a.out_vals);
+    const uint32_t lane = threadIdx.x & 31, q = lane & (G - 1), grp = lane / G;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    constexpr uint32_t RPW = 32 / G;  // rows per warp
+    // base is the same in the whole warp, so every lane reaches every shuffle
+    for (uint64_t base = warp * RPW; base < a.n; base += nwarps * RPW) {
+        const uint64_t i = base + grp;
+        bool act = i < a.n;
+        uint32_t beg = 0, len = 0, dst = 0;
+        if (act) {
+            const uint32_t src = a.perm[i];
+            if (src >= a.n) {
+                act = false;  // reported by k_perm_rowlen
+            } else {
+                beg = a.rp[src];
+                len = a.rp[src + 1] - beg;
+                dst = a.out_rp[i];
+                if (dst > a.nnz || len > a.nnz - dst || beg > a.nnz || len > a.nnz - beg) {
+                    if (q == 0)
+                        fail(a.res, 311);  // not a permutation: the rows do not tile the output
+                    act = false;
+                } else if (len > G) {
+                    if (q == 0)
+                        mid[atomicAdd(counters, 1u)] = (uint32_t)i;  // at most n rows: the list holds n
+                    act = false;
+                }
+            }
+        }
+        const bool mine = act && q < len;
+        uint32_t key = 0xFFFFFFFFu;
+        if (mine) {
+            const uint32_t c = a.ci[beg + q];
+            key = c < a.n ? a.inv[c] : 0xFFFFFFFFu;
+        }
+        uint32_t r = 0;
+#pragma unroll
+        for (uint32_t t = 0; t < G; ++t) {
+            const uint32_t kt = __shfl_sync(0xFFFFFFFFu, key, (lane & ~(G - 1)) + t);
+            r += (t < len) && ((kt < key) || (kt == key && t < q));
+        }
+        if (mine) {
+            a.out_ci[dst + r] = key;
+            if (out_vals)
+                out_vals[dst + r] = vals[beg + q];
+            if (a.out_map)
+                a.out_map[dst + r] = beg + q;
+        }
+    }
+}
+
+// Listed rows of B by one warp each (rows of at most kWarpRow entries);
+// longer rows are listed for k_permute_long.
+template <typename V>
+__global__ void __launch_bounds__(kRowWarps * 32) k_permute_rows(PermView a, const uint32_t* mid,
+                                                                 const uint32_t* counters, uint32_t* long_rows,
+                                                                 uint32_t cap_long, uint32_t* nlong)
 {
     __shared__ uint32_t keys[kRowWarps][kWarpRow];
     const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t* kw = keys[w];
     const V* vals = static_cast<const V*>(a.vals);
     V* out_vals = static_cast<V*>(a.out_vals);
-    for (uint64_t i = (uint64_t)blockIdx.x * kRowWarps + w; i < a.n; i += (uint64_t)gridDim.x * kRowWarps) {
+    const uint32_t nmid = min(counters[0], a.n);
+    for (uint32_t r0 = blockIdx.x * kRowWarps + w; r0 < nmid; r0 += gridDim.x * kRowWarps) {
+        const uint32_t i = mid[r0];
         const uint32_t src = a.perm[i];
-        if (src >= a.n)
-            continue;  // reported by k_perm_rowlen
         const uint32_t beg = a.rp[src], len = a.rp[src + 1] - beg, dst = a.out_rp[i];
-        if (dst > a.nnz || len > a.nnz - dst || beg > a.nnz || len > a.nnz - beg) {
-            if (lane == 0)
-                fail(a.res, 311);  // not a permutation: the rows do not tile the output
-            continue;
-        }
         if (len > (uint32_t)kWarpRow) {
             if (lane == 0) {
                 const uint32_t k = atomicAdd(nlong, 1u);
@@ -316,11 +375,13 @@ __global__ void __launch_bounds__(kLongThreads) k_permute_long(PermView a, const
 }
 
 template <typename V>
-cudaError_t launch_rows(const PermView& a, uint32_t* long_rows, uint32_t cap_long, uint32_t* nlong,
+cudaError_t launch_rows(const PermView& a, uint32_t* mid, uint32_t* counters, uint32_t* long_rows, uint32_t cap_long,
                         uint32_t* scratch, int sms, cudaStream_t st)
 {
-    const int blocks = (int)std::min<uint64_t>(((uint64_t)a.n + kRowWarps - 1) / kRowWarps, (uint64_t)sms * 8);
-    k_permute_rows<V><<<blocks < 1 ? 1 : blocks, kRowWarps * 32, 0, st>>>(a, long_rows, cap_long, nlong);
+    uint32_t* nlong = counters + 1;
+    const int sb = (int)std::min<uint64_t>(((uint64_t)a.n + 31) / 32, (uint64_t)sms * 16);
+    k_permute_short<V><<<sb < 1 ? 1 : sb, 256, 0, st>>>(a, mid, counters);
+    k_permute_rows<V><<<sms * 4, kRowWarps * 32, 0, st>>>(a, mid, counters, long_rows, cap_long, nlong);
     if (scratch != nullptr && cap_long > 0) {
         uint32_t bits = 1;
         while (bits < 32 && (a.n - 1u) >> bits)
@@ -335,16 +396,16 @@ cudaError_t launch_rows(const PermView& a, uint32_t* long_rows, uint32_t cap_lon
 
 cudaError_t launch_permute(const uint32_t* rp, const uint32_t* ci, const void* vals, uint32_t val_bytes, uint32_t n,
                            uint32_t nnz, const uint32_t* perm, uint32_t* inv, uint32_t* out_rp, uint32_t* out_ci,
-                           void* out_vals, uint32_t* out_map, uint32_t* partials, uint32_t* long_rows,
-                           uint32_t cap_long, uint32_t* nlong, uint32_t* scratch, DevResult* res, int sms,
-                           cudaStream_t st)
+                           void* out_vals, uint32_t* out_map, uint32_t* partials, uint32_t* mid_rows,
+                           uint32_t* long_rows, uint32_t cap_long, uint32_t* counters, uint32_t* scratch,
+                           DevResult* res, int sms, cudaStream_t st)
 {
     int blocks = (int)std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)sms * 8);
     if (blocks < 1)
         blocks = 1;
     cudaError_t e = cudaMemsetAsync(inv, 0xFF, sizeof(uint32_t) * (size_t)n, st);
     if (e == cudaSuccess)
-        e = cudaMemsetAsync(nlong, 0, sizeof(uint32_t), st);
+        e = cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), st);
     if (e != cudaSuccess)
         return e;
     launch_perm_inverse(perm, n, inv, res, blocks, st);
@@ -357,8 +418,29 @@ cudaError_t launch_permute(const uint32_t* rp, const uint32_t* ci, const void* v
     PermView a{rp, ci, val_bytes ? vals : nullptr, perm, inv, out_rp, out_ci, val_bytes ? out_vals : nullptr,
                out_map, n, nnz, res};
     if (val_bytes == 8)
-        return launch_rows<unsigned long long>(a, long_rows, cap_long, nlong, scratch, sms, st);
-    return launch_rows<uint32_t>(a, long_rows, cap_long, nlong, scratch, sms, st);
+        return launch_rows<unsigned long long>(a, mid_rows, counters, long_rows, cap_long, scratch, sms, st);
+    return launch_rows<uint32_t>(a, mid_rows, counters, long_rows, cap_long, scratch, sms, st);
+}
+
+cudaError_t launch_permute_long(const uint32_t* rp, const uint32_t* ci, const void* vals, uint32_t val_bytes,
+                                uint32_t n, uint32_t nnz, const uint32_t* perm, const uint32_t* inv,
+                                const uint32_t* out_rp, uint32_t* out_ci, void* out_vals, uint32_t* out_map,
+                                const uint32_t* long_rows, uint32_t cap_long, const uint32_t* counters,
+                                uint32_t* scratch, DevResult* res, int sms, cudaStream_t st)
+{
+    PermView a{rp, ci, val_bytes ? vals : nullptr, perm, inv, out_rp, out_ci, val_bytes ? out_vals : nullptr,
+               out_map, n, nnz, res};
+    uint32_t bits = 1;
+    while (bits < 32 && (n - 1u) >> bits)
+        ++bits;
+    const uint32_t passes = (bits + 7) / 8;
+    if (val_bytes == 8)
+        k_permute_long<unsigned long long><<<sms, kLongThreads, 0, st>>>(a, long_rows, counters + 1, cap_long,
+                                                                         scratch, passes);
+    else
+        k_permute_long<uint32_t><<<sms, kLongThreads, 0, st>>>(a, long_rows, counters + 1, cap_long, scratch,
+                                                               passes);
+    return cudaGetLastError();
 }
 
 uint32_t scan_partials_count(uint32_t n)

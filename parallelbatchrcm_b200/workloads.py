@@ -253,7 +253,68 @@ def run_serve(args, ws, rank, local):
     return 0
 
 
+def run_permute(args, ws, rank, local):
+    """The reordered matrix B = P A P^T of the 128^3 grid (float64 values, its
+    RCM order) through pbrcm_permute_device, device-resident, L2 flushed
+    between steps; reports permutes/s and the HBM bytes the call must move."""
+    import torch
+
+    import parallelbatchrcm_b200 as P
+    from parallelbatchrcm_b200 import gen
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    m = gen.grid3d(128, 128, 128, seed=12345)
+    n, nnz = m.n, m.nnz
+    ctx = P.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    rp = torch.from_numpy(m.row_ptr.view(np.int32)).to(dev)
+    ci = torch.from_numpy(m.col_idx.view(np.int32)).to(dev)
+    vals = torch.rand(nnz, dtype=torch.float64, device=dev)
+    perm, _ = P.reorder_device(rp, ci, reverse=True, ctx=ctx)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=dev)
+
+    def step():
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = P.permute_device(rp, ci, perm, vals, ctx=ctx, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    ms = [step()[0] for _ in range(args.steps)]
+    ms_med = statistics.median(ms)
+    # inputs row_ptr, col_idx, values, perm; outputs row_ptr, col_idx, values
+    abytes = 4 * (n + 1) + 4 * nnz + 8 * nnz + 4 * n + 4 * (n + 1) + 4 * nnz + 8 * nnz
+    peak = None
+    try:
+        with open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                               "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f).get("hbm_gbs"))
+    except (OSError, ValueError, TypeError):
+        peak = None
+    achieved = abytes / (ms_med / 1e3) / 1e9
+    line = {
+        "metric": "permutes/s (B = P A P^T, float64 values)", "value": 1e3 / ms_med, "unit": "permutes/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_med, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32+f64", "data": "synthetic (seeded 128^3 grid, RCM order)",
+        "config": {"workload": "grid3d_128^3_permute_f64", "n": n, "nnz": nnz,
+                   "l2": "flushed (256 MiB write) between steps"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "algorithmic_bytes": abytes,
+                     "includes": "the CSR check and one stream synchronisation of the call"},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(args, ws, rank, local):
+    if args.workload == "permute":
+        return run_permute(args, ws, rank, local)
     if args.workload == "batch":
         return run_batch(args, ws, rank, local)
     if args.workload == "serve":

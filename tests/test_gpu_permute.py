@@ -122,3 +122,19 @@ def test_oracle_matches_cusolver_csrperm(oracle_mod):
     finally:
         sp.cusparseDestroyMatDescr(descr)
         sol.cusolverSpDestroy(handle)
+
+
+def test_permute_long_row_on_a_fresh_context(pbrcm, oracle_mod):
+    """A row of 3,000 entries on a context that has no scratch yet: the
+    long-row pass runs after the scratch is allocated."""
+    g = load_golden("star_3000")
+    ctx = pbrcm.Context(0)
+    try:
+        vals = np.arange(g["col_idx"].shape[0], dtype=np.float32)
+        for _ in range(2):
+            orp, oci, ov, om = pbrcm.permute(g["row_ptr"], g["col_idx"], g["perm"], vals, want_map=True, ctx=ctx)
+            erp, eci, ev, em = oracle_mod.permute_csr(g["row_ptr"], g["col_idx"], g["perm"], vals)
+            assert np.array_equal(orp, erp) and np.array_equal(oci, eci) and np.array_equal(om, em)
+            assert np.array_equal(ov, ev)
+    finally:
+        ctx.close()
