@@ -261,6 +261,20 @@ PBRCM_API int32_t pbrcm_prepare_csr(const uint32_t* row_ptr, const uint32_t* col
 
 PBRCM_API void pbrcm_free(void* p);
 
+/*
+ * The reference's binary CSR cache, `.hicsr` (storeCSR / loadCSR,
+ * src/CSR.cpp:57-168; Graph<T>::load keeps `<file>.hicsr` and
+ * `<file>.rcm.hicsr` next to a MatrixMarket input, include/Graph.h:266-332).
+ * pbrcm_load_hicsr reads either; *row_ptr, *col_idx and (if vals is not NULL)
+ * *vals are malloc'd (free with pbrcm_free), *val_bytes is 4 (float) or 8
+ * (double).  pbrcm_store_hicsr writes one the reference can read; without
+ * values (val_bytes 0) every value is float 1.0.
+ */
+PBRCM_API int32_t pbrcm_load_hicsr(const char* path, uint32_t* n, uint64_t* nnz, uint32_t** row_ptr,
+                                   uint32_t** col_idx, void** vals, uint32_t* val_bytes);
+PBRCM_API int32_t pbrcm_store_hicsr(const char* path, uint32_t n, uint64_t nnz, const uint32_t* row_ptr,
+                                    const uint32_t* col_idx, const void* vals, uint32_t val_bytes);
+
 /* ---------------------------------------------------------------------- */
 /* Output boundary: the reordered matrix (the reference's `-o`).           */
 /* ---------------------------------------------------------------------- */

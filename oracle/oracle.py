@@ -273,3 +273,23 @@ def ref_store_mtx(rp, ci, vals, path: str) -> None:
         mode = "store64" if v.dtype == np.float64 else "store32"
         subprocess.run([REF_BIN, mode, os.path.join(td, "rp"), os.path.join(td, "ci"), os.path.join(td, "v"), path],
                        capture_output=True, text=True, check=True)
+
+
+def ref_read_hicsr(path: str, dtype):
+    """The reference's loadCSR<float|double> on a .hicsr file: (rp, ci, vals)."""
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "o")
+        mode = "hicsr64" if np.dtype(dtype) == np.float64 else "hicsr32"
+        subprocess.run([REF_BIN, mode, path, out], capture_output=True, text=True, check=True)
+        return (np.fromfile(out + ".rp", dtype=np.uint32), np.fromfile(out + ".ci", dtype=np.uint32),
+                np.fromfile(out + ".v", dtype=dtype))
+
+
+def ref_load_caches(mtx_path: str, workdir: str):
+    """Runs the reference's Graph<float>::load on a copy of `mtx_path` in
+    `workdir`; returns the paths of the .hicsr and .rcm.hicsr caches it wrote
+    (include/Graph.h:266-332)."""
+    src = os.path.join(workdir, "m.mtx")
+    shutil.copyfile(mtx_path, src)
+    subprocess.run([REF_BIN, "load", src, os.path.join(workdir, "out")], capture_output=True, text=True, check=True)
+    return src + ".hicsr", src + ".rcm.hicsr"

@@ -17,6 +17,9 @@
 //   ref_rcm store64|store32 <rp> <ci> <vals> <out.mtx>
 //       CSR<double|float> with the given values -> convert(COO, CSR)
 //       (CSR.cpp:210-231) -> storeMTX (COO.cpp:213-251).
+//   ref_rcm hicsr32|hicsr64 <file.hicsr> <outprefix>
+//       loadCSR<float|double> (CSR.cpp:119-151), dumped to <outprefix>.rp /
+//       .ci / .v.
 //   ref_rcm time <rp> <ci> <threads> <steps>
 //       Times <steps> reorders: findPeripheral + RealCPU::rcm<true> with
 //       <threads> workers (1 = the serial rcm_seq path, else CPU_BATCH with
@@ -153,6 +156,17 @@ int analyze(Graph<float>& g, const std::string& outprefix, long forced_start)
 }  // namespace
 
 template <typename T>
+int dumpHicsr(const char* file, const std::string& out)
+{
+    CSR<T> csr = loadCSR<T>(file);
+    writeU32(out + ".rp", csr.row_offsets.get(), csr.rows + 1);
+    writeU32(out + ".ci", csr.col_ids.get(), csr.nnz);
+    std::ofstream fv(out + ".v", std::ios::binary);
+    fv.write(reinterpret_cast<const char*>(csr.data.get()), static_cast<std::streamsize>(csr.nnz * sizeof(T)));
+    return 0;
+}
+
+template <typename T>
 int storeAs(const std::vector<uint32_t>& rp, const std::vector<uint32_t>& ci, std::ifstream& fv, const char* out)
 {
     const size_t n = rp.size() - 1;
@@ -198,6 +212,11 @@ int main(int argc, char** argv)
             if (std::strcmp(argv[1], "store64") == 0)
                 return storeAs<double>(rp, ci, fv, argv[5]);
             return storeAs<float>(rp, ci, fv, argv[5]);
+        }
+        if (argc >= 4 && (std::strcmp(argv[1], "hicsr32") == 0 || std::strcmp(argv[1], "hicsr64") == 0)) {
+            if (std::strcmp(argv[1], "hicsr64") == 0)
+                return dumpHicsr<double>(argv[2], argv[3]);
+            return dumpHicsr<float>(argv[2], argv[3]);
         }
         if (argc >= 6 && std::strcmp(argv[1], "time") == 0) {
             Graph<float> g;

@@ -348,6 +348,111 @@ int32_t pbrcm_prepare_csr(const uint32_t* row_ptr, const uint32_t* col_idx, uint
 
 void pbrcm_free(void* p) { std::free(p); }
 
+// The reference's binary CSR cache (.hicsr, src/CSR.cpp:57-168): a header
+// of a 9-byte magic and eight u64 fields (type size, compressed direction,
+// index size, fixed offset, offset size, rows, columns, non-zeros), the
+// State<T> {scaling, transpose} record, then values, column ids, row offsets.
+namespace {
+const char kHiMagic[9] = {'H', 'i', 1, 'C', 'o', 'm', 'p', 's', 'd'};
+struct HiHeader {
+    char magic[9];
+    char pad[7];
+    uint64_t typesize, compresseddir, indexsize, fixedoffset, offsetsize, rows, cols, nnz;
+};
+static_assert(sizeof(HiHeader) == 80, "hicsr header layout");
+size_t hi_state_bytes(uint64_t typesize) { return typesize == 8 ? 16 : 8; }  // {T scaling; bool transpose}
+}  // namespace
+
+int32_t pbrcm_load_hicsr(const char* path, uint32_t* n, uint64_t* nnz, uint32_t** row_ptr, uint32_t** col_idx,
+                         void** vals, uint32_t* val_bytes)
+{
+    if (!path || !n || !nnz || !row_ptr || !col_idx)
+        return PBRCM_ERR_ARG;
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f)
+        return PBRCM_ERR_NOT_FOUND;
+    HiHeader h;
+    unsigned char state[16];
+    int32_t rc = PBRCM_OK;
+    uint32_t *rp = nullptr, *ci = nullptr;
+    void* v = nullptr;
+    if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, kHiMagic, 9) != 0 ||
+        (h.typesize != 4 && h.typesize != 8) || h.indexsize != 4 || h.offsetsize != 4 || h.compresseddir != 0 ||
+        h.rows != h.cols || h.rows == 0 || h.rows >= 0xFFFFFFFFull || h.nnz > 0xFFFFFFF0ull ||
+        std::fread(state, hi_state_bytes(h.typesize), 1, f) != 1) {
+        rc = PBRCM_ERR_FORMAT;
+    } else {
+        rp = static_cast<uint32_t*>(std::malloc(4 * (h.rows + 1)));
+        ci = static_cast<uint32_t*>(std::malloc(4 * std::max<uint64_t>(h.nnz, 1)));
+        v = std::malloc(h.typesize * std::max<uint64_t>(h.nnz, 1));
+        if (!rp || !ci || !v)
+            rc = PBRCM_ERR_OOM;
+        else if (std::fread(v, h.typesize, h.nnz, f) != h.nnz || std::fread(ci, 4, h.nnz, f) != h.nnz ||
+                 std::fread(rp, 4, h.rows + 1, f) != h.rows + 1)
+            rc = PBRCM_ERR_FORMAT;
+        else if (rp[0] != 0 || rp[h.rows] != h.nnz)
+            rc = PBRCM_ERR_FORMAT;
+    }
+    std::fclose(f);
+    if (rc != PBRCM_OK) {
+        std::free(rp);
+        std::free(ci);
+        std::free(v);
+        return rc;
+    }
+    *n = (uint32_t)h.rows;
+    *nnz = h.nnz;
+    *row_ptr = rp;
+    *col_idx = ci;
+    if (vals) {
+        *vals = v;
+    } else {
+        std::free(v);
+    }
+    if (val_bytes)
+        *val_bytes = (uint32_t)h.typesize;
+    return PBRCM_OK;
+}
+
+int32_t pbrcm_store_hicsr(const char* path, uint32_t n, uint64_t nnz, const uint32_t* row_ptr, const uint32_t* col_idx,
+                          const void* vals, uint32_t val_bytes)
+{
+    if (!path || !row_ptr || (!col_idx && nnz) || (val_bytes != 0 && val_bytes != 4 && val_bytes != 8) ||
+        (val_bytes && nnz && !vals) || row_ptr[n] != nnz)
+        return PBRCM_ERR_ARG;
+    HiHeader h;
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, kHiMagic, 9);
+    h.typesize = val_bytes ? val_bytes : 4;  // no values: float 1.0, the reference's pattern data
+    h.indexsize = 4;
+    h.offsetsize = 4;
+    h.rows = h.cols = n;
+    h.nnz = nnz;
+    unsigned char state[16];
+    std::memset(state, 0, sizeof(state));
+    if (h.typesize == 8) {
+        const double one = 1.0;
+        std::memcpy(state, &one, 8);
+    } else {
+        const float one = 1.0f;
+        std::memcpy(state, &one, 4);
+    }
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f)
+        return PBRCM_ERR_IO;
+    bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1 && std::fwrite(state, hi_state_bytes(h.typesize), 1, f) == 1;
+    if (ok && val_bytes) {
+        ok = std::fwrite(vals, val_bytes, nnz, f) == nnz;
+    } else if (ok) {
+        const float one = 1.0f;
+        for (uint64_t k = 0; k < nnz && ok; ++k)
+            ok = std::fwrite(&one, 4, 1, f) == 1;
+    }
+    ok = ok && std::fwrite(col_idx, 4, nnz, f) == nnz && std::fwrite(row_ptr, 4, (size_t)n + 1, f) == (size_t)n + 1;
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? PBRCM_OK : PBRCM_ERR_IO;
+}
+
 int32_t pbrcm_store_mtx(const char* path, uint32_t n, uint64_t nnz, const uint32_t* row_ptr, const uint32_t* col_idx,
                         const void* vals, uint32_t val_bytes)
 {

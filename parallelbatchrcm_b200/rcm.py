@@ -33,7 +33,7 @@ __all__ = [
     "PbrcmError", "Context", "default_options", "reorder", "reorder_device", "reorder_device_noalloc",
     "find_peripheral",
     "bandwidth", "reorder_batch", "reorder_batch_device", "Session", "load_mtx", "prepare_csr", "permute",
-    "permute_device", "store_mtx",
+    "permute_device", "store_mtx", "load_hicsr", "store_hicsr",
     "Graph", "GPU_BATCH", "SimplePeripheral", "compute_bandwidth", "check_bandwidth", "max_valency",
     "check_permutation", "AUTO_START", "DEBUG_PHANTOM_CTA",
 ]
@@ -368,6 +368,31 @@ def permute_device(row_ptr_t, col_idx_t, perm_t, vals_t=None, *, want_map: bool 
         vb, n, nnz, perm_t.data_ptr(), orp.data_ptr(), oci.data_ptr(), ov.data_ptr() if ov is not None else None,
         om.data_ptr() if om is not None else None, st), "pbrcm_permute_device")
     return orp, oci[:nnz], (ov[:nnz] if ov is not None else None), (om[:nnz] if om is not None else None)
+
+
+def load_hicsr(path: str):
+    """(row_ptr, col_idx, values) of a reference `.hicsr` CSR cache
+    (src/CSR.cpp:57-168); values float32 or float64 as stored."""
+    L = _lib.lib()
+    n, nnz, vb = ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint32()
+    rp_p, ci_p = ctypes.POINTER(ctypes.c_uint32)(), ctypes.POINTER(ctypes.c_uint32)()
+    v_p = ctypes.c_void_p()
+    _check(L.pbrcm_load_hicsr(path.encode(), ctypes.byref(n), ctypes.byref(nnz), ctypes.byref(rp_p),
+                              ctypes.byref(ci_p), ctypes.byref(v_p), ctypes.byref(vb)), f"pbrcm_load_hicsr({path})")
+    dt = np.float64 if vb.value == 8 else np.float32
+    buf = (ctypes.c_char * (vb.value * max(nnz.value, 1))).from_address(v_p.value)
+    vals = np.frombuffer(buf, dtype=dt)[:nnz.value].copy()
+    L.pbrcm_free(v_p)
+    rp, ci = _take_csr(n.value, nnz.value, rp_p, ci_p)
+    return rp, ci, vals
+
+
+def store_hicsr(path: str, row_ptr, col_idx, vals=None):
+    """Writes a `.hicsr` CSR cache the reference's loadCSR reads."""
+    rp, ci = _u32(row_ptr), _u32(col_idx)
+    v, vb = _vals(vals)
+    _check(_lib.lib().pbrcm_store_hicsr(path.encode(), rp.shape[0] - 1, ci.shape[0], _ptr(rp), _ptr(ci),
+                                        _ptr(v) if v is not None else None, vb), f"pbrcm_store_hicsr({path})")
 
 
 def store_mtx(path: str, row_ptr, col_idx, vals=None):
