@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/pbrcm.h"
@@ -29,19 +30,54 @@ struct CsrBuf {
     std::vector<uint32_t> rp, ci;
 };
 
-// COO (row, col) pairs -> CSR sorted by (row, col), duplicates kept.
-void coo_to_csr(uint32_t n, std::vector<uint64_t>& keys, CsrBuf& out)
+// Sorts each row's columns (rows are short: insertion sort; long rows:
+// std::sort).
+void sort_rows(CsrBuf& out)
 {
-    std::sort(keys.begin(), keys.end());
+    for (uint32_t r = 0; r < out.n; ++r) {
+        uint32_t* b = out.ci.data() + out.rp[r];
+        uint32_t* e = out.ci.data() + out.rp[r + 1];
+        if (e - b > 32) {
+            std::sort(b, e);
+            continue;
+        }
+        for (uint32_t* i = b + 1; i < e; ++i) {
+            const uint32_t v = *i;
+            uint32_t* j = i;
+            while (j > b && *(j - 1) > v) {
+                *j = *(j - 1);
+                --j;
+            }
+            *j = v;
+        }
+    }
+}
+
+// COO (row, col) pairs, in one or more runs -> CSR sorted by (row, col),
+// duplicates kept: a counting sort by row, then each row's columns sorted.
+void coo_to_csr(uint32_t n, const std::vector<const std::vector<uint64_t>*>& runs, CsrBuf& out)
+{
     out.n = n;
     out.rp.assign((size_t)n + 1, 0);
-    out.ci.resize(keys.size());
-    for (size_t i = 0; i < keys.size(); ++i) {
-        out.ci[i] = (uint32_t)(keys[i] & 0xFFFFFFFFull);
-        out.rp[(keys[i] >> 32) + 1]++;
+    size_t total = 0;
+    for (const auto* run : runs) {
+        total += run->size();
+        for (uint64_t k : *run)
+            out.rp[(k >> 32) + 1]++;
     }
     for (uint32_t i = 0; i < n; ++i)
         out.rp[i + 1] += out.rp[i];
+    out.ci.resize(total);
+    std::vector<uint32_t> fill(out.rp.begin(), out.rp.end() - 1);
+    for (const auto* run : runs)
+        for (uint64_t k : *run)
+            out.ci[fill[k >> 32]++] = (uint32_t)(k & 0xFFFFFFFFull);
+    sort_rows(out);
+}
+
+void coo_to_csr(uint32_t n, std::vector<uint64_t>& keys, CsrBuf& out)
+{
+    coo_to_csr(n, std::vector<const std::vector<uint64_t>*>{&keys}, out);
 }
 
 inline uint64_t pair_key(uint32_t r, uint32_t c)
@@ -182,6 +218,8 @@ inline bool parse_u64(const char*& p, const char* e, unsigned long long& v)
     return true;
 }
 
+// A value token must read as one number up to the next white space (the
+// buffer ends in a NUL, so strtod stops at the latest there).
 inline bool skip_number(const char*& p, const char* e)
 {
     p = skip_ws(p, e);
@@ -191,9 +229,41 @@ inline bool skip_number(const char*& p, const char* e)
     if (p == s)
         return false;
     char* end = nullptr;
-    std::string tok(s, p);
-    std::strtod(tok.c_str(), &end);
-    return end && *end == '\0';
+    std::strtod(s, &end);
+    return end == p;
+}
+
+// Body lines [b, e) (b at a line start) -> (row, col) keys; counts entries.
+struct ParseOut {
+    std::vector<uint64_t> coo;
+    unsigned long long entries = 0;
+    int32_t rc = PBRCM_OK;
+};
+
+void parse_body(const char* b, const char* e, bool pattern, bool sym, unsigned long long nr, ParseOut& o)
+{
+    const char* p = b;
+    while (p < e) {
+        const char* nl = static_cast<const char*>(std::memchr(p, '\n', (size_t)(e - p)));
+        const char* le = nl ? nl : e;
+        const char* ls = p;
+        p = nl ? nl + 1 : e;
+        if (ls < le && *ls == '%')
+            continue;
+        const char* q = skip_ws(ls, le);
+        if (q >= le)
+            continue;
+        unsigned long long r, c;
+        if (!parse_u64(q, le, r) || !parse_u64(q, le, c) || (!pattern && !skip_number(q, le)) || r == 0 || c == 0 ||
+            r > nr || c > nr) {
+            o.rc = PBRCM_ERR_FORMAT;
+            return;
+        }
+        ++o.entries;
+        o.coo.push_back(((r - 1) << 32) | (c - 1));
+        if (sym && r != c)
+            o.coo.push_back(((c - 1) << 32) | (r - 1));
+    }
 }
 
 int32_t load_mtx(const char* path, CsrBuf& out)
@@ -256,28 +326,44 @@ int32_t load_mtx(const char* path, CsrBuf& out)
     }
     if (nr != nc || nr == 0 || nr >= 0xFFFFFFFFull)
         return PBRCM_ERR_FORMAT;
-    std::vector<uint64_t> coo;
-    coo.reserve((size_t)nz * ((symmetric || hermitian) ? 2 : 1));
-    unsigned long long entries = 0;
-    while (next_line(ls, le)) {
-        if (ls < le && *ls == '%')
-            continue;
-        const char* q = skip_ws(ls, le);
-        if (q >= le)
-            continue;
-        unsigned long long r, c;
-        if (!parse_u64(q, le, r) || !parse_u64(q, le, c))
-            return PBRCM_ERR_FORMAT;
-        if (!pattern && !skip_number(q, le))
-            return PBRCM_ERR_FORMAT;
-        if (r == 0 || c == 0 || r > nr || c > nc || entries >= nz)
-            return PBRCM_ERR_FORMAT;
-        ++entries;
-        coo.push_back(((r - 1) << 32) | (c - 1));
-        if ((symmetric || hermitian) && r != c)
-            coo.push_back(((c - 1) << 32) | (r - 1));
+    // the body in parallel: chunks of whole lines, one thread each
+    const size_t body = (size_t)(e - p);
+    unsigned threads = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (body < (1u << 20))
+        threads = 1;
+    std::vector<const char*> cut(threads + 1);
+    cut[0] = p;
+    cut[threads] = e;
+    for (unsigned t = 1; t < threads; ++t) {
+        const char* c = p + body * t / threads;
+        c = std::max(c, cut[t - 1]);
+        const char* nl = c < e ? static_cast<const char*>(std::memchr(c, '\n', (size_t)(e - c))) : nullptr;
+        cut[t] = nl ? nl + 1 : e;
     }
-    coo_to_csr((uint32_t)nr, coo, out);
+    std::vector<ParseOut> parts(threads);
+    const bool sym = symmetric || hermitian;
+    for (unsigned t = 0; t < threads; ++t)
+        parts[t].coo.reserve((size_t)((cut[t + 1] - cut[t]) / 8) * (sym ? 2 : 1));
+    if (threads == 1) {
+        parse_body(cut[0], cut[1], pattern, sym, nr, parts[0]);
+    } else {
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < threads; ++t)
+            pool.emplace_back(parse_body, cut[t], cut[t + 1], pattern, sym, nr, std::ref(parts[t]));
+        for (auto& th : pool)
+            th.join();
+    }
+    unsigned long long entries = 0;
+    std::vector<const std::vector<uint64_t>*> runs;
+    for (auto& part : parts) {
+        if (part.rc != PBRCM_OK)
+            return part.rc;
+        entries += part.entries;
+        runs.push_back(&part.coo);
+    }
+    if (entries > nz)
+        return PBRCM_ERR_FORMAT;  // more entries than the size line declares
+    coo_to_csr((uint32_t)nr, runs, out);
     return prepare(out, !symmetric);
 }
 
