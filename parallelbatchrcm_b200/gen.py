@@ -229,6 +229,19 @@ def mixed_batch_specs(count: int = 4096, nmin: int = 500, nmax: int = 200_000, s
     return specs
 
 
+def spec_nnz_estimate(spec) -> int:
+    """Approximate nnz of a spec's matrix without building it (for sharding)."""
+    kind, dims, _ = spec
+    if kind == "grid2d":
+        a, b = dims[0], dims[1]
+        return 5 * a * b - 2 * (a + b)
+    if kind == "grid3d":
+        a, b, c = dims[0], dims[1], dims[2]
+        return 7 * a * b * c - 2 * (a * b + b * c + a * c)
+    n, kmin, kmax = dims
+    return int(n * (1 + 1.5 * (kmin + kmax) / 2))
+
+
 def make_from_spec(spec) -> Csr:
     kind, dims, seed = spec
     if kind == "grid2d":

@@ -64,3 +64,18 @@ def test_reference_arm_under_torchrun_two_ranks():
     assert len(lines) == 1, r.stdout
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_batch_shards_by_nnz():
+    sys.path.insert(0, ROOT)
+    from parallelbatchrcm_b200 import gen, workloads
+    specs = gen.mixed_batch_specs(count=300, seed=42)
+    est = [gen.spec_nnz_estimate(s) for s in specs]
+    shards = workloads.shard_by_nnz(est, 3)
+    assert sorted(i for s in shards for i in s) == list(range(300))
+    loads = [sum(est[i] for i in s) for s in shards]
+    assert max(loads) - min(loads) <= max(est)  # longest-first greedy bound
+    # the estimate is close to the real count
+    for s in specs[:20]:
+        real = gen.make_from_spec(s).nnz
+        assert 0.7 * real <= gen.spec_nnz_estimate(s) <= 1.4 * real, (s, real)
