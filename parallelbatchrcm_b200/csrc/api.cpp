@@ -156,7 +156,7 @@ Context::~Context()
         cudaSetDevice(device);
     if (stream)
         cudaStreamSynchronize(stream);
-    for (void* p : {(void*)d_pw, (void*)d_rp, (void*)d_ci, (void*)d_node, (void*)d_perm, (void*)d_rec, (void*)d_rec2, (void*)d_hub,
+    for (void* p : {(void*)d_pw, (void*)d_rp, (void*)d_ci, (void*)d_node, (void*)d_perm, (void*)d_rec, (void*)d_rec2, (void*)d_stage, (void*)d_hub,
                     (void*)d_res, (void*)d_gs, (void*)d_agg, (void*)d_jobs, (void*)d_slots, (void*)d_counter, (void*)d_bres,
                     (void*)d_arena})
         if (p)
@@ -196,7 +196,7 @@ bool Context::ensure_single(uint32_t n, uint64_t nnz, bool inputs)
     if (inputs && (!grow(d_rp, cap_rp, (size_t)n + 1) || !grow(d_ci, cap_ci, (size_t)nnz)))
         return false;
     return grow(d_node, cap_node, n) && grow(d_rec, cap_rec, n) && grow(d_rec2, cap_rec2, n) &&
-           grow(d_perm, cap_perm, n);
+           grow(d_stage, cap_stage, std::max<uint64_t>(nnz, 1)) && grow(d_perm, cap_perm, n);
 }
 
 bool Context::ensure_hub(uint64_t nnz) { return grow(d_hub, cap_hub, 4 * (size_t)std::max<uint64_t>(nnz, 1)); }
@@ -216,6 +216,7 @@ int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
         M.node = d_node;
         M.rec = d_rec;
         M.rec2 = d_rec2;
+        M.stage = d_stage;
         M.perm = perm;
         M.hub = with_hub ? d_hub : nullptr;
         M.res = d_res;

@@ -985,6 +985,53 @@ struct Chunk {
         }
     }
 
+    // Writes the ranked children of the chunk to M.stage[at..]: node, row
+    // start, valence and the child-edge offset eoff0 + so_eoff[i].
+    __device__ void stage_children(uint32_t at, uint32_t eoff0)
+    {
+        const uint32_t Q = s.Q;
+        for (uint32_t i = threadIdx.x; i < Q; i += B) {
+            const uint32_t x = s.so_idx[i];
+            if (PB_CHECK(M.res, (uint64_t)at + i < M.nnz, 130))
+                __stcg(reinterpret_cast<uint4*>(M.stage) + at + i,
+                       make_uint4(s.ch_node[x], s.ch_rs[x], s.ch_deg[x], eoff0 + s.so_eoff[i]));
+        }
+    }
+
+    // Places the `count` children staged at M.stage[at..] (in order) at
+    // positions P0.. with edge ids K0 + their child-edge offsets, and claims
+    // their edges, in tiles of up to EMAX children.
+    __device__ void place_staged(uint32_t at, uint32_t count, uint32_t P0, uint32_t K0, bool write_perm,
+                                 bool reverse)
+    {
+        uint32_t done = 0, kdone = 0;
+        while (done < count) {
+            const uint32_t cnt = min((uint32_t)EMAX, count - done);
+            for (uint32_t i = threadIdx.x; i < cnt; i += B) {
+                uint4 r = make_uint4(0u, 0u, 0u, kdone);
+                if (PB_CHECK(M.res, (uint64_t)at + done + i < M.nnz, 131))
+                    r = __ldcg(reinterpret_cast<const uint4*>(M.stage) + at + done + i);
+                s.ch_node[i] = r.x;
+                s.ch_rs[i] = r.y;
+                s.ch_deg[i] = r.z;
+                s.so_idx[i] = i;
+                s.so_eoff[i] = r.w - kdone;
+                if (i == cnt - 1) {
+                    s.so_eoff[cnt] = r.w + r.z - kdone;
+                    s.Q = cnt;
+                    s.Qdeg = r.w + r.z - kdone;
+                    s.npre = 0;
+                }
+            }
+            __syncthreads();
+            const uint32_t qdeg = s.Qdeg;
+            place_and_claim(P0 + done, K0 + kdone, write_perm, reverse);
+            __syncthreads();
+            done += cnt;
+            kdone += qdeg;
+        }
+    }
+
     // ---- hubs: one parent with more than EMAX edges -----------------------
     // Scratch layout (4 arrays of nnz words): key0 | val0 | key1 | val1.  A
     // hub at level-relative edge offset r0 owns [r0, r0 + deg) of each.
@@ -1322,18 +1369,30 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, uns
         const uint32_t F = st.b - st.a;
         const uint32_t p_beg = st.a + (uint32_t)(((uint64_t)F * R) / G);
         const uint32_t p_end = st.a + (uint32_t)(((uint64_t)F * (R + 1)) / G);
-        // A1: collect and count
+        // A1: collect and count.  A CTA whose parents take several chunks
+        // stages each chunk's ranked children (M.stage, at the level-relative
+        // edge offset of its first parent: the CTAs' regions are disjoint and
+        // hold their children, which are at most their parents' edges), so
+        // that placing them needs no second collect.
         uint32_t my_cnt = 0, my_esum = 0, nunits = 0;
         bool last_hub = false;
+        bool staged = M.stage != nullptr;  // every unit staged (no hub among them)
+        uint32_t stage_base = 0;
         uint32_t p = p_beg;
         while (p < p_end) {
             const uint32_t used = ch.form(p, p_end);
+            if (nunits == 0)
+                stage_base = s.peb[0] - st.Ka;
             Agg g;
             last_hub = s.hub != 0;
-            if (last_hub)
+            if (last_hub) {
                 g = ch.hub_collect(s.peb[0] - st.Ka, sorted);
-            else
+                staged = false;
+            } else {
                 g = ch.collect(sorted);
+                if (staged && !(nunits == 0 && used == p_end - p))
+                    ch.stage_children(stage_base + my_cnt, my_esum);
+            }
             my_cnt += g.cnt;
             my_esum += g.esum;
             ++nunits;
@@ -1354,9 +1413,11 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, uns
         const uint32_t tot_esum = (uint32_t)(all >> 32);
         uint32_t P = st.b + (uint32_t)(pre & 0xFFFFFFFFull);
         uint32_t K = st.Kb + (uint32_t)(pre >> 32);
-        // A2: place (the only unit is still in shared memory)
+        // A2: place (the only unit is still in shared memory, or all are staged)
         if (keep) {
             ch.place_and_claim(P, K, write_perm, reverse);
+        } else if (nunits > 0 && staged) {
+            ch.place_staged(stage_base, my_cnt, P, K, write_perm, reverse);
         } else if (nunits > 0) {
             p = p_beg;
             while (p < p_end) {
@@ -1493,6 +1554,7 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& tea
     MatrixView M2 = M;  // the speculative ordered pass's view
     M2.rec = M.rec2;
     M2.cf = 3;
+    M2.stage = nullptr;  // the other half stages in M.stage
     bool spec_on = false;    // speculation chosen after the first pass
     bool spec_done = false;  // the speculative ordered pass wrote the output
 
