@@ -60,6 +60,7 @@ void apply_team_shape(const Context& C, Options& opt)
     opt.solo_edges = C.solo_edges;
     opt.solo_parents = C.solo_parents;
     opt.barrier = C.barrier;
+    opt.spec_from = C.spec_from;
 }
 
 void fill_result(const DevResult& r, const Options& opt, pbrcm_result* out)
@@ -133,6 +134,7 @@ int32_t Context::init(int dev)
     solo_parents = (uint32_t)env_int("PBRCM_SOLO_PARENTS", kVariants[team_variant].block);
     solo_edges = (uint32_t)env_int("PBRCM_SOLO_EDGES", kVariants[team_variant].emax);
     barrier = (uint32_t)env_int("PBRCM_BARRIER", 0) ? 1u : 0u;
+    spec_from = (uint32_t)std::max(0, env_int("PBRCM_SPEC_FROM", 3));
     batch_variant = env_int("PBRCM_BATCH_VARIANT", 2);
     if (batch_variant < 0 || batch_variant >= kNumVariants)
         batch_variant = 2;

@@ -23,6 +23,7 @@ struct Context {
     uint32_t solo_edges = 0;    // levels at most this big run on one CTA
     uint32_t solo_parents = 0;
     uint32_t barrier = 0;       // team barrier implementation
+    uint32_t spec_from = 3;     // speculative split from this search pass on (team-dominated matrices)
     int team_maxc = 0;          // co-resident CTAs of the team kernel
     // batches: the biggest matrices go to thread-block-cluster teams
     int cluster_size = 2;             // CTAs per cluster (0 or 1: off)

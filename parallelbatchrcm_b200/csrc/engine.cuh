@@ -1234,7 +1234,8 @@ struct Chunk {
 template <int B, int EMAX, class TeamT>
 __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, unsigned long long* agg,
                          uint32_t& step, const Options& opt, uint32_t start, uint32_t base, bool sorted,
-                         bool write_perm, bool reverse, uint32_t& placed, uint32_t& nlevels, uint32_t& last_start)
+                         bool write_perm, bool reverse, uint32_t& placed, uint32_t& nlevels, uint32_t& last_start,
+                         uint32_t& wide_f, uint32_t& wide_e)
 {
     Chunk<B, EMAX> ch{s, M, base};
     const uint32_t t = threadIdx.x;
@@ -1367,6 +1368,8 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, uns
         }
         // ---- whole team ---------------------------------------------------
         const uint32_t F = st.b - st.a;
+        wide_f = max(wide_f, F);
+        wide_e = max(wide_e, st.Kb - st.Ka);
         const uint32_t p_beg = st.a + (uint32_t)(((uint64_t)F * R) / G);
         const uint32_t p_end = st.a + (uint32_t)(((uint64_t)F * (R + 1)) / G);
         // A1: collect and count.  A CTA whose parents take several chunks
@@ -1555,7 +1558,9 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& tea
     M2.rec = M.rec2;
     M2.cf = 3;
     M2.stage = nullptr;  // the other half stages in M.stage
-    bool spec_on = false;    // speculation chosen after the first pass
+    bool spec_on = false;    // the next search pass runs beside the speculative ordered pass
+    bool solo_dom = false;   // most levels of the first pass ran on one CTA
+    bool narrow = false;     // every team level of the first pass is narrow enough for a half team
     bool spec_done = false;  // the speculative ordered pass wrote the output
 
     // pseudo-peripheral search (simple_peripheral.cpp:92-141), then the
@@ -1595,9 +1600,9 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& tea
         ++pid;
         const uint32_t base = pid * kspan + M.nnz + 1u;
         const uint32_t step0 = step;
-        uint32_t pl = 0, nl = 0, ls = 0;
+        uint32_t pl = 0, nl = 0, ls = 0, wf = 0, we = 0;
         if (!bfs_pass<B, EMAX>(s, spec_half ? M2 : M, tm, ag, stp, opt, start, base, ordered, ordered,
-                               ordered && opt.reverse != 0, pl, nl, ls))
+                               ordered && opt.reverse != 0, pl, nl, ls, wf, we))
             return;
         if (!searching) {
             placed = pl;
@@ -1612,10 +1617,17 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& tea
                     set_status(M.res, kErrDisconnected, 0);
                 return;
             }
-            // speculate only if at most a quarter of the levels needed the
-            // whole team (step counts them)
-            if (passes == 1)
-                spec_on = spec && 4ull * (step - step0) <= nl;
+            // speculate from the next pass on if at most a quarter of the
+            // levels needed the whole team (step counts them); otherwise from
+            // pass opt.spec_from on, where the search usually ends, if the
+            // widest level takes a CTA of a half team at most four chunks
+            // (measured: the 128^3 grid, 1.6 chunks, gains 14 %; a 1M-node
+            // RGG, 20 chunks, would lose 30 %)
+            if (passes == 1) {
+                solo_dom = 4ull * (step - step0) <= nl;
+                narrow = (uint64_t)wf <= 4ull * half * B && (uint64_t)we <= 4ull * half * EMAX;
+            }
+            spec_on = spec && (solo_dom || (narrow && opt.spec_from != 0 && passes + 1 >= opt.spec_from));
             dist = nl - 1;
             if (dist == lastdist) {
                 ecc = dist;

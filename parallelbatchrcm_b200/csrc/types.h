@@ -131,7 +131,7 @@ struct Options {
     uint32_t solo_edges;    // a level with at most this many edges runs on CTA 0 alone
     uint32_t solo_parents;  // ... and at most this many parents
     uint32_t barrier;       // team barrier: 0 counter, 1 flag array
-    uint32_t pad;
+    uint32_t spec_from;     // speculative split from this search pass on (0: only for solo-dominated matrices)
 };
 
 constexpr uint32_t kModeFull = 0;
