@@ -198,7 +198,7 @@ bool Context::ensure_single(uint32_t n, uint64_t nnz, bool inputs)
     if (inputs && (!grow(d_rp, cap_rp, (size_t)n + 1) || !grow(d_ci, cap_ci, (size_t)nnz)))
         return false;
     return grow(d_node, cap_node, n) && grow(d_rec, cap_rec, n) && grow(d_rec2, cap_rec2, n) &&
-           grow(d_stage, cap_stage, std::max<uint64_t>(nnz, 1)) && grow(d_perm, cap_perm, n);
+           grow(d_stage, cap_stage, 2 * std::max<uint64_t>(nnz, 1)) && grow(d_perm, cap_perm, n);
 }
 
 bool Context::ensure_hub(uint64_t nnz) { return grow(d_hub, cap_hub, 4 * (size_t)std::max<uint64_t>(nnz, 1)); }

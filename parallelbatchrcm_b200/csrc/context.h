@@ -44,7 +44,7 @@ struct Context {
     size_t cap_rec = 0;
     PosRec* d_rec2 = nullptr;  // queue records of the speculative ordered pass
     size_t cap_rec2 = 0;
-    PosRec* d_stage = nullptr;  // staged children of multi-chunk team levels (nnz)
+    PosRec* d_stage = nullptr;  // staged children of multi-chunk team levels (2 nnz)
     size_t cap_stage = 0;
     uint32_t* d_hub = nullptr;
     size_t cap_hub = 0;

@@ -1557,7 +1557,7 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& tea
     MatrixView M2 = M;  // the speculative ordered pass's view
     M2.rec = M.rec2;
     M2.cf = 3;
-    M2.stage = nullptr;  // the other half stages in M.stage
+    M2.stage = M.stage != nullptr ? M.stage + M.nnz : nullptr;  // its own half of the staging array
     bool spec_on = false;    // the next search pass runs beside the speculative ordered pass
     bool solo_dom = false;   // most levels of the first pass ran on one CTA
     bool narrow = false;     // every team level of the first pass is narrow enough for a half team

@@ -82,7 +82,8 @@ struct MatrixView {
     DevResult* res;
     PosRec* rec2;                      // n: queue records of the speculative ordered pass, or nullptr
     uint32_t cf;                       // claim word of NodeEntry this pass uses (0 claim, 3 inv)
-    PosRec* stage;                     // nnz: ranked children of multi-chunk team levels, or nullptr
+    PosRec* stage;                     // 2 nnz: ranked children of multi-chunk team levels (the
+                                       // speculative half uses the second nnz), or nullptr
 };
 
 constexpr uint64_t kMaxNnz = 0xFFFFFFF0ull;
