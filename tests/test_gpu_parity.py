@@ -197,3 +197,17 @@ def test_session_results_equal_single(pbrcm, gpu_ctx):
             assert res["status"] == 0 and np.array_equal(perm, q) and res["bandwidth"] == s["bandwidth"]
         st = sess.stats()
         assert st["completed"] == len(mats) and st["p99_ms"] >= st["p50_ms"] > 0
+
+
+@pytest.mark.parametrize("case", ["grid3d_128", "rgg_1M"])
+def test_full_size_configs_match_oracle(pbrcm, gpu_ctx, oracle_mod, case):
+    """The benchmark configurations at full size (128^3 grid, 2.1M nodes;
+    1M-node RGG): start, passes, permutation, bandwidth and profile exact."""
+    from parallelbatchrcm_b200 import gen
+    m = gen.grid3d(128, 128, 128, seed=12345) if case == "grid3d_128" else gen.rgg(1_000_000, seed=7)
+    perm, res = pbrcm.reorder(m.row_ptr, m.col_idx, reverse=True, ctx=gpu_ctx)
+    ref = oracle_mod.full_reorder(m.row_ptr, m.col_idx, reverse=True)
+    assert (res["start_node"], res["peripheral_passes"], res["eccentricity"]) == (
+        ref["start"], ref["passes"], ref["ecc"])
+    assert np.array_equal(perm, ref["perm"])
+    assert res["bandwidth"] == ref["bandwidth"] and res["profile"] == ref["profile"]
