@@ -303,6 +303,30 @@ PBRCM_API int32_t pbrcm_permute_device(pbrcm_context* ctx, const uint32_t* d_row
                                        void* d_vals_out, uint32_t* d_map_out, void* stream);
 
 /*
+ * The connectivity repair of the reference's loader (Graph<T>::prepareRCM,
+ * include/Graph.h:160-263) on device buffers: every component is joined to
+ * the rest by the links that loader adds -- with minn the first non-empty
+ * row, (m - 1, m) for each component whose smallest node m > 0 is not in
+ * minn's, and (0, minn) when row 0 is empty -- both directions inserted at
+ * their sorted place.  The input is the symmetric pattern the loader has at
+ * that point (every row sorted by column, as pbrcm_load_mtx and the
+ * reference's convert leave it); a column out of range, an unsorted row or a
+ * missing transposed entry returns PBRCM_ERR_ARG, a matrix without entries
+ * PBRCM_ERR_FORMAT.  An empty row is a component of its own (the reference
+ * never finishes on one; pbrcm_prepare_csr links it the same way).
+ * Outputs: d_row_ptr_out (n + 1) and d_col_idx_out (cap_nnz_out entries;
+ * nnz + 2 (n - 1) always suffices); *nnz_out = the output's entry count and
+ * *links_out (nullable) = the links added.  A connected matrix comes back
+ * unchanged.  With cap_nnz_out below *nnz_out the call returns PBRCM_ERR_ARG
+ * with *nnz_out set (the output is incomplete; call again with room).
+ * Enqueued on `stream` (NULL = the context's stream), synchronised before
+ * returning.
+ */
+PBRCM_API int32_t pbrcm_connect_device(pbrcm_context* ctx, const uint32_t* d_row_ptr, const uint32_t* d_col_idx,
+                                       uint32_t n, uint64_t nnz, uint32_t* d_row_ptr_out, uint32_t* d_col_idx_out,
+                                       uint64_t cap_nnz_out, uint64_t* nnz_out, uint32_t* links_out, void* stream);
+
+/*
  * Writes a CSR as a MatrixMarket file in the reference's format (storeMTX,
  * src/COO.cpp:213-251: "coordinate real general", 1-based "row col value"
  * lines, values printed like std::to_string).  val_bytes 4 = float, 8 =

@@ -8,7 +8,8 @@ by hand-written CUDA kernels behind the C ABI of include/pbrcm.h
 """
 from .rcm import (  # noqa: F401
     AUTO_START, DEBUG_PHANTOM_CTA, GPU_BATCH, Context, Graph, PbrcmError, Session, SimplePeripheral, bandwidth,
-    check_bandwidth, check_permutation, compute_bandwidth, default_options, find_peripheral, load_hicsr, load_mtx,
+    check_bandwidth, check_permutation, compute_bandwidth, connect_device, default_options, find_peripheral,
+    load_hicsr, load_mtx,
     max_valency, store_hicsr,
     permute, permute_device, prepare_csr, reorder, reorder_batch, reorder_batch_device, reorder_device,
     reorder_device_noalloc, store_mtx,

@@ -104,6 +104,8 @@ SIGNATURES = {
     "pbrcm_free": (None, [_vp]),
     "pbrcm_permute": (_i32, [_vp, _vp, _vp, _vp, _u32, _u32, _u64, _vp, _vp, _vp, _vp, _vp]),
     "pbrcm_permute_device": (_i32, [_vp, _vp, _vp, _vp, _u32, _u32, _u64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pbrcm_connect_device": (_i32, [_vp, _vp, _vp, _u32, _u64, _vp, _vp, _u64, ctypes.POINTER(ctypes.c_uint64),
+                                    _pu32, _vp]),
     "pbrcm_store_mtx": (_i32, [ctypes.c_char_p, _u32, _u64, _vp, _vp, _vp, _u32]),
     "pbrcm_load_hicsr": (_i32, [ctypes.c_char_p, _pu32, ctypes.POINTER(ctypes.c_uint64),
                                 ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)),

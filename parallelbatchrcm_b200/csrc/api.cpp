@@ -304,6 +304,44 @@ int32_t Context::run_permute(const uint32_t* rp, const uint32_t* ci, const void*
     return map_status(h_res->status);
 }
 
+// parent (n) | scan partials | counters
+size_t Context::connect_work_bytes(uint32_t n)
+{
+    return al256(4 * (size_t)n) + al256(4 * (size_t)scan_partials_count(n)) + 256;
+}
+
+// The loader's connectivity repair into out_* after the CSR check on the same
+// stream (the repair kernels clamp every row range themselves); one
+// synchronisation of `st`.
+int32_t Context::run_connect(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint64_t nnz, uint32_t* out_rp,
+                             uint32_t* out_ci, uint64_t cap, uint64_t* nnz_out, uint32_t* links_out,
+                             unsigned char* work, cudaStream_t st)
+{
+    uint32_t* parent = reinterpret_cast<uint32_t*>(work);
+    uint32_t* partials = reinterpret_cast<uint32_t*>(work + al256(4 * (size_t)n));
+    uint32_t* counters =
+        reinterpret_cast<uint32_t*>(work + al256(4 * (size_t)n) + al256(4 * (size_t)scan_partials_count(n)));
+    if (cudaMemsetAsync(d_res, 0, sizeof(DevResult), st) != cudaSuccess ||
+        launch_validate(rp, ci, n, (uint32_t)nnz, d_res, sms, st) != cudaSuccess ||
+        launch_connect(rp, ci, n, (uint32_t)nnz, out_rp, out_ci, cap, parent, partials, counters, sms, st) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(h_res, d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(h_aux, counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return PBRCM_ERR_CUDA;
+    if (h_res->status != kOk)
+        return map_status(h_res->status);
+    if (h_aux[2] != 0)
+        return PBRCM_ERR_ARG;  // column out of range, unsorted row or not symmetric
+    if (h_aux[0] >= n)
+        return PBRCM_ERR_FORMAT;  // no entry at all
+    const uint64_t need = nnz + 2ull * h_aux[1];
+    *nnz_out = need;
+    if (links_out)
+        *links_out = h_aux[1];
+    return need > kMaxNnz || need > cap ? PBRCM_ERR_ARG : PBRCM_OK;
+}
+
 static int32_t check_sizes(uint32_t n, uint64_t nnz)
 {
     if (n == 0 || n == 0xFFFFFFFFu || nnz > kMaxNnz)
@@ -486,6 +524,25 @@ int32_t pbrcm_permute_device(pbrcm_context* ctx, const uint32_t* d_row_ptr, cons
     cudaStream_t st = stream ? (cudaStream_t)stream : C.stream;
     return C.run_permute(d_row_ptr, d_col_idx, d_vals, val_bytes, n, nnz, d_perm, d_row_ptr_out, d_col_idx_out,
                          d_vals_out, d_map_out, C.d_pw, st);
+}
+
+int32_t pbrcm_connect_device(pbrcm_context* ctx, const uint32_t* d_row_ptr, const uint32_t* d_col_idx, uint32_t n,
+                             uint64_t nnz, uint32_t* d_row_ptr_out, uint32_t* d_col_idx_out, uint64_t cap_nnz_out,
+                             uint64_t* nnz_out, uint32_t* links_out, void* stream)
+{
+    if (!d_row_ptr || (!d_col_idx && nnz) || !d_row_ptr_out || (!d_col_idx_out && cap_nnz_out) || !nnz_out)
+        return PBRCM_ERR_ARG;
+    if (int32_t rc = check_sizes(n, nnz))
+        return rc;
+    if (nnz == 0)
+        return PBRCM_ERR_FORMAT;
+    PBRCM_CTX(ctx);
+    Context& C = ctx->ctx;
+    if (!grow(C.d_pw, C.cap_pw, Context::connect_work_bytes(n)))
+        return PBRCM_ERR_OOM;
+    cudaStream_t st = stream ? (cudaStream_t)stream : C.stream;
+    return C.run_connect(d_row_ptr, d_col_idx, n, nnz, d_row_ptr_out, d_col_idx_out, cap_nnz_out, nnz_out, links_out,
+                         C.d_pw, st);
 }
 
 int32_t pbrcm_permute(pbrcm_context* ctx, const uint32_t* row_ptr, const uint32_t* col_idx, const void* vals,

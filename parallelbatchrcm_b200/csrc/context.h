@@ -78,6 +78,10 @@ struct Context {
                         uint64_t nnz, const uint32_t* perm, uint32_t* out_rp, uint32_t* out_ci, void* out_vals,
                         uint32_t* out_map, unsigned char* work, cudaStream_t st);
     static size_t permute_work_bytes(uint32_t n, uint64_t nnz);
+    int32_t run_connect(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint64_t nnz, uint32_t* out_rp,
+                        uint32_t* out_ci, uint64_t cap, uint64_t* nnz_out, uint32_t* links_out, unsigned char* work,
+                        cudaStream_t st);
+    static size_t connect_work_bytes(uint32_t n);
     int32_t run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint64_t nnz, uint32_t* perm,
                        const Options& opt, cudaStream_t st, DevResult* out, float* dev_ms);
 };

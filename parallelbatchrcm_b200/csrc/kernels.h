@@ -59,6 +59,17 @@ cudaError_t launch_permute_long(const uint32_t* rp, const uint32_t* ci, const vo
                                 const uint32_t* long_rows, uint32_t cap_long, const uint32_t* counters,
                                 uint32_t* scratch, DevResult* res, int sms, cudaStream_t st);
 uint32_t scan_partials_count(uint32_t n);
+// in-place inclusive scan of data[0..m) (permute.cu); partials holds
+// scan_partials_count(m) words
+cudaError_t launch_scan(uint32_t* data, uint64_t m, uint32_t* partials, cudaStream_t st);
+// The loader's connectivity repair (connect.cu): out_rp (n+1) and out_ci
+// (writes at or past cap dropped) from a symmetric CSR with sorted rows.
+// Workspace: parent (n), partials (scan_partials_count(n)), counters (4):
+// [0] first non-empty row, [1] links added, [2] check flags (1 column out of
+// range, 2 row not sorted, 4 not symmetric, 8 union limit).
+cudaError_t launch_connect(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint32_t nnz, uint32_t* out_rp,
+                           uint32_t* out_ci, uint64_t cap, uint32_t* parent, uint32_t* partials, uint32_t* counters,
+                           int sms, cudaStream_t st);
 uint32_t permute_long_cap(uint32_t n, uint64_t nnz);
 constexpr uint32_t kPermuteWarpRow = 1024;  // longest row of the warp path
 cudaError_t launch_bandwidth(const uint32_t* rp, const uint32_t* ci, uint32_t n, const uint32_t* perm, uint32_t* inv,

@@ -394,6 +394,18 @@ cudaError_t launch_rows(const PermView& a, uint32_t* mid, uint32_t* counters, ui
 
 }  // namespace
 
+cudaError_t launch_scan(uint32_t* data, uint64_t m, uint32_t* partials, cudaStream_t st)
+{
+    const uint64_t per = (uint64_t)kScanThreads * kScanItems;
+    const uint32_t nb = (uint32_t)((m + per - 1) / per);
+    if (nb == 0)
+        return cudaSuccess;
+    k_scan_local<<<nb, kScanThreads, 0, st>>>(data, m, partials);
+    k_scan_partials<<<1, kScanThreads, 0, st>>>(partials, nb);
+    k_scan_add<<<nb, kScanThreads, 0, st>>>(data, m, partials);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_permute(const uint32_t* rp, const uint32_t* ci, const void* vals, uint32_t val_bytes, uint32_t n,
                            uint32_t nnz, const uint32_t* perm, uint32_t* inv, uint32_t* out_rp, uint32_t* out_ci,
                            void* out_vals, uint32_t* out_map, uint32_t* partials, uint32_t* mid_rows,
@@ -410,11 +422,9 @@ cudaError_t launch_permute(const uint32_t* rp, const uint32_t* ci, const void* v
         return e;
     launch_perm_inverse(perm, n, inv, res, blocks, st);
     k_perm_rowlen<<<blocks, 256, 0, st>>>(rp, perm, n, out_rp, res);
-    const uint64_t per = (uint64_t)kScanThreads * kScanItems;
-    const uint32_t nb = (uint32_t)(((uint64_t)n + per - 1) / per);
-    k_scan_local<<<nb, kScanThreads, 0, st>>>(out_rp + 1, n, partials);
-    k_scan_partials<<<1, kScanThreads, 0, st>>>(partials, nb);
-    k_scan_add<<<nb, kScanThreads, 0, st>>>(out_rp + 1, n, partials);
+    e = launch_scan(out_rp + 1, n, partials, st);
+    if (e != cudaSuccess)
+        return e;
     PermView a{rp, ci, val_bytes ? vals : nullptr, perm, inv, out_rp, out_ci, val_bytes ? out_vals : nullptr,
                out_map, n, nnz, res};
     if (val_bytes == 8)

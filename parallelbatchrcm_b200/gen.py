@@ -144,11 +144,12 @@ def grid3d(nx: int, ny: int, nz: int, seed: int | None = 12345) -> Csr:
     return m
 
 
-def rgg(n: int, kmin: int = 6, kmax: int = 14, long_frac: float = 0.001, seed: int = 7) -> Csr:
+def rgg(n: int, kmin: int = 6, kmax: int = 14, long_frac: float = 0.001, seed: int = 7,
+        connect: bool = True) -> Csr:
     """Random geometric graph: n points uniform in [0,1]^2, point i joined to
     its k_i ~ U{kmin..kmax} nearest neighbours, symmetrised, plus
     round(long_frac * |E|) uniformly random long-range edges; labels shuffled;
-    components joined by the loader's rule."""
+    components joined by the loader's rule (connect=False: left apart)."""
     from scipy.spatial import cKDTree
 
     rng = np.random.default_rng(seed)
@@ -169,8 +170,10 @@ def rgg(n: int, kmin: int = 6, kmax: int = 14, long_frac: float = 0.001, seed: i
     u = np.concatenate([e // n, a])
     v = np.concatenate([e % n, b])
     u, v = _relabel(n, u, v, seed + 1)
-    m = connect_components(from_edges(n, u, v))
-    m.name = f"rgg_{n}_k{kmin}-{kmax}_s{seed}"
+    m = from_edges(n, u, v)
+    if connect:
+        m = connect_components(m)
+    m.name = f"rgg_{n}_k{kmin}-{kmax}_s{seed}" + ("" if connect else "_raw")
     return m
 
 

@@ -32,7 +32,8 @@ from ._lib import AUTO_START, DEBUG_PHANTOM_CTA, Matrix, Options, Result, Sessio
 __all__ = [
     "PbrcmError", "Context", "default_options", "reorder", "reorder_device", "reorder_device_noalloc",
     "find_peripheral",
-    "bandwidth", "reorder_batch", "reorder_batch_device", "Session", "load_mtx", "prepare_csr", "permute",
+    "bandwidth", "reorder_batch", "reorder_batch_device", "Session", "load_mtx", "prepare_csr", "connect_device",
+    "permute",
     "permute_device", "store_mtx", "load_hicsr", "store_hicsr",
     "Graph", "GPU_BATCH", "SimplePeripheral", "compute_bandwidth", "check_bandwidth", "max_valency",
     "check_permutation", "AUTO_START", "DEBUG_PHANTOM_CTA",
@@ -368,6 +369,34 @@ def permute_device(row_ptr_t, col_idx_t, perm_t, vals_t=None, *, want_map: bool 
         vb, n, nnz, perm_t.data_ptr(), orp.data_ptr(), oci.data_ptr(), ov.data_ptr() if ov is not None else None,
         om.data_ptr() if om is not None else None, st), "pbrcm_permute_device")
     return orp, oci[:nnz], (ov[:nnz] if ov is not None else None), (om[:nnz] if om is not None else None)
+
+
+def connect_device(row_ptr_t, col_idx_t, *, cap: int | None = None, ctx: Context | None = None, stream=None):
+    """The loader's connectivity repair (Graph<T>::prepareRCM,
+    include/Graph.h:160-263) on device-resident torch tensors of a symmetric
+    pattern with sorted rows.  Returns (row_ptr, col_idx, links): the joined
+    CSR on the same device and the number of links added.  The output is
+    first given room for `cap` entries (default: nnz plus a small slack) and
+    reallocated to the exact size if the matrix needs more."""
+    import torch
+
+    n, nnz = row_ptr_t.numel() - 1, col_idx_t.numel()
+    dev = row_ptr_t.device
+    orp = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    room = cap if cap is not None else nnz + 2 * min(max(n - 1, 0), max(1024, n // 64))
+    st = stream.cuda_stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    L = _lib.lib()
+    for _ in range(2):
+        oci = torch.empty(max(room, 1), dtype=torch.int32, device=dev)
+        got, links = ctypes.c_uint64(0), ctypes.c_uint32(0)
+        rc = L.pbrcm_connect_device(_h(ctx), row_ptr_t.data_ptr(), col_idx_t.data_ptr(), n, nnz, orp.data_ptr(),
+                                    oci.data_ptr(), room, ctypes.byref(got), ctypes.byref(links), st)
+        if rc == 1 and got.value > room:  # PBRCM_ERR_ARG with the size needed: too little room
+            room = got.value
+            continue
+        _check(rc, "pbrcm_connect_device")
+        return orp, oci[:got.value], links.value
+    raise PbrcmError(1, "pbrcm_connect_device: output size changed between calls")
 
 
 def load_hicsr(path: str):

@@ -348,7 +348,113 @@ def run_permute(args, ws, rank, local):
     return 0
 
 
+def run_connect(args, ws, rank, local):
+    """The loader's connectivity repair on the device (pbrcm_connect_device)
+    for the 1M-node random geometric graph before it is joined (the same
+    generator as the rgg configuration, its components left apart); inputs
+    device-resident, L2 flushed between steps.  e2e: the host CSR copied in,
+    joined, and the joined CSR copied back every step.  cpu_baseline: the
+    oracle's restatement of the reference's repair on one host core."""
+    import torch
+
+    import parallelbatchrcm_b200 as P
+    from parallelbatchrcm_b200 import gen
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    m = gen.rgg(1_000_000, connect=False)
+    n, nnz = m.n, m.nnz
+    ctx = P.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    rp = torch.from_numpy(m.row_ptr.view(np.int32)).to(dev)
+    ci = torch.from_numpy(m.col_idx.view(np.int32)).to(dev)
+    _, oci, links = P.connect_device(rp, ci, ctx=ctx, stream=stream)
+    cap = oci.numel()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=dev)
+
+    def step():
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        P.connect_device(rp, ci, cap=cap, ctx=ctx, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    ms_med = statistics.median([step() for _ in range(args.steps)])
+
+    h_rp = torch.from_numpy(m.row_ptr.view(np.int32)).pin_memory()
+    h_ci = torch.from_numpy(m.col_idx.view(np.int32)).pin_memory()
+    o_rp = torch.empty(n + 1, dtype=torch.int32).pin_memory()
+    o_ci = torch.empty(cap, dtype=torch.int32).pin_memory()
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        with torch.cuda.stream(stream):
+            d_rp = h_rp.to(dev, non_blocking=True)
+            d_ci = h_ci.to(dev, non_blocking=True)
+        orp, oci2, _ = P.connect_device(d_rp, d_ci, cap=cap, ctx=ctx, stream=stream)
+        with torch.cuda.stream(stream):
+            o_rp.copy_(orp, non_blocking=True)
+            o_ci[:oci2.numel()].copy_(oci2, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(3):
+        e2e_step()
+    e2e_ms = statistics.median([e2e_step() for _ in range(args.steps)])
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+        import oracle as O
+        t0 = time.perf_counter()
+        reps = 0
+        while reps < 3 or time.perf_counter() - t0 < 2.0:
+            O.prepare_csr(m.row_ptr, m.col_idx, check_sym=False)
+            reps += 1
+        cpu_s = (time.perf_counter() - t0) / reps
+        cpu = {"value": 1.0 / cpu_s, "unit": "connects/s", "cores": 1, "kind": "port",
+               "sample": f"{reps} full repairs of the same graph"}
+
+    nnz_out = nnz + 2 * links
+    # row_ptr and col_idx in and out, the parent array written and read once
+    abytes = 4 * (n + 1) + 4 * nnz + 4 * (n + 1) + 4 * nnz_out + 8 * n
+    peak = None
+    try:
+        with open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                               "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f).get("hbm_gbs"))
+    except (OSError, ValueError, TypeError):
+        peak = None
+    achieved = abytes / (ms_med / 1e3) / 1e9
+    line = {
+        "metric": "connects/s (loader connectivity repair)", "value": 1e3 / ms_med, "unit": "connects/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_med, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded RGG, components apart)",
+        "config": {"workload": "rgg_1M_raw_connect", "n": n, "nnz": nnz, "links": links,
+                   "l2": "flushed (256 MiB write) between steps"},
+        "e2e": {"value": 1e3 / e2e_ms, "unit": "connects/s", "h2d_bytes_per_step": 4 * (n + 1) + 4 * nnz,
+                "d2h_bytes_per_step": 4 * (n + 1) + 4 * nnz_out},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "algorithmic_bytes": abytes,
+                     "includes": "the CSR check and one stream synchronisation of the call"},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(args, ws, rank, local):
+    if args.workload == "connect":
+        return run_connect(args, ws, rank, local)
     if args.workload == "permute":
         return run_permute(args, ws, rank, local)
     if args.workload == "batch":
