@@ -166,7 +166,7 @@ def prepare_csr(rp, ci, check_sym: bool = True):
 
 
 def full_reorder(rp, ci, start: int | None = None, reverse: bool = True):
-    """What the drop-in returns: (perm, start, bandwidth, profile, passes, ecc)
+    """What the drop-in returns: {perm, start, bandwidth, profile, passes, ecc}
     with automatic start unless given, CM order reversed when `reverse`."""
     passes = ecc = 0
     if start is None:

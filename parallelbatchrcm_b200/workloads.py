@@ -350,8 +350,9 @@ def run_permute(args, ws, rank, local):
 
 def run_connect(args, ws, rank, local):
     """The loader's connectivity repair on the device (pbrcm_connect_device)
-    for the 1M-node random geometric graph before it is joined (the same
-    generator as the rgg configuration, its components left apart); inputs
+    for a 4M-node random geometric graph of 1-3 nearest neighbours per point
+    (about 160k components; the rgg generator with its components left
+    apart); inputs
     device-resident, L2 flushed between steps.  e2e: the host CSR copied in,
     joined, and the joined CSR copied back every step.  cpu_baseline: the
     oracle's restatement of the reference's repair on one host core."""
@@ -362,7 +363,7 @@ def run_connect(args, ws, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    m = gen.rgg(1_000_000, connect=False)
+    m = gen.rgg(4_000_000, kmin=1, kmax=3, long_frac=0.0, connect=False)
     n, nnz = m.n, m.nnz
     ctx = P.Context(local)
     stream = torch.cuda.Stream(device=dev)
@@ -439,7 +440,7 @@ def run_connect(args, ws, rank, local):
         "metric": "connects/s (loader connectivity repair)", "value": 1e3 / ms_med, "unit": "connects/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_med, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded RGG, components apart)",
-        "config": {"workload": "rgg_1M_raw_connect", "n": n, "nnz": nnz, "links": links,
+        "config": {"workload": "rgg_4M_k1-3_connect", "n": n, "nnz": nnz, "links": links,
                    "l2": "flushed (256 MiB write) between steps"},
         "e2e": {"value": 1e3 / e2e_ms, "unit": "connects/s", "h2d_bytes_per_step": 4 * (n + 1) + 4 * nnz,
                 "d2h_bytes_per_step": 4 * (n + 1) + 4 * nnz_out},

@@ -51,17 +51,20 @@ def test_connected_matrix_unchanged(pbrcm, gpu_ctx):
     assert links == 0 and np.array_equal(arp, m.row_ptr) and np.array_equal(aci, m.col_idx)
 
 
-def test_raw_rgg_1m_matches_oracle(pbrcm, gpu_ctx, oracle_mod):
-    """The 1M-node random geometric graph before the loader joins it (the
-    long-range edges leave some hundred small components), and a reorder of
-    the joined matrix against the oracle's RCM of the oracle's join."""
+def test_sparse_rgg_1m_matches_oracle(pbrcm, gpu_ctx, oracle_mod):
+    """A 1M-node random geometric graph of 1-3 nearest neighbours per point
+    before the loader joins it (about 40k components), the generator's own
+    join, and a reorder of the joined matrix against the oracle."""
     from parallelbatchrcm_b200 import gen
-    m = gen.rgg(1_000_000, connect=False)
+    m = gen.rgg(1_000_000, kmin=1, kmax=3, long_frac=0.0, connect=False)
     links = _check(pbrcm, gpu_ctx, oracle_mod, m.row_ptr, m.col_idx)
-    assert links > 0
-    j = gen.rgg(1_000_000)
+    assert links > 10_000
+    j = gen.connect_components(m)
     arp, aci, _ = _run(pbrcm, gpu_ctx, m.row_ptr, m.col_idx)
     assert np.array_equal(arp, j.row_ptr) and np.array_equal(aci, j.col_idx)
+    perm, res = pbrcm.reorder(arp, aci, reverse=True, ctx=gpu_ctx)
+    eperm = oracle_mod.full_reorder(arp, aci)["perm"]
+    assert np.array_equal(perm, eperm)
 
 
 def test_forest_of_small_trees(pbrcm, gpu_ctx, oracle_mod):
