@@ -92,6 +92,9 @@ typedef struct pbrcm_result {
     uint64_t profile;            /* of the result (0 if not asked) */
     float device_ms;             /* device time of the reorder launch(es) */
     float total_ms;              /* host wall time of the call */
+    uint32_t engine;             /* 0: team engine (one cooperative launch); 1: level-synchronous
+                                    engine for wide, shallow graphs (same result) */
+    uint32_t reserved;
 } pbrcm_result;
 
 /* Default options: reverse=1, automatic start, stable=1, want_bandwidth=1. */

@@ -37,7 +37,8 @@ class Result(ctypes.Structure):
         ("status", ctypes.c_int32), ("start_node", ctypes.c_uint32), ("peripheral_passes", ctypes.c_uint32),
         ("eccentricity", ctypes.c_uint32), ("levels", ctypes.c_uint32), ("placed", ctypes.c_uint32),
         ("bandwidth", ctypes.c_int64), ("initial_bandwidth", ctypes.c_int64), ("profile", ctypes.c_uint64),
-        ("device_ms", ctypes.c_float), ("total_ms", ctypes.c_float),
+        ("device_ms", ctypes.c_float), ("total_ms", ctypes.c_float), ("engine", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:

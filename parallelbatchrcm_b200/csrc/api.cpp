@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -73,6 +74,7 @@ void fill_result(const DevResult& r, const Options& opt, pbrcm_result* out)
     out->eccentricity = r.ecc;
     out->levels = r.levels;
     out->placed = r.placed;
+    out->engine = r.engine;
     if (opt.want_bw && r.status == kOk && opt.mode == kModeFull) {
         out->bandwidth = (int64_t)r.bandwidth;
         out->initial_bandwidth = (int64_t)r.initial_bw;
@@ -135,6 +137,13 @@ int32_t Context::init(int dev)
     solo_edges = (uint32_t)env_int("PBRCM_SOLO_EDGES", kVariants[team_variant].emax);
     barrier = (uint32_t)env_int("PBRCM_BARRIER", 0) ? 1u : 0u;
     spec_from = (uint32_t)std::max(0, env_int("PBRCM_SPEC_FROM", 3));
+    // wide, shallow graphs: PBRCM_WIDE_DIV (0: never), PBRCM_WIDE_MIN,
+    // PBRCM_ENGINE=wide to run the level-synchronous engine first
+    wide_div = (uint32_t)std::max(0, env_int("PBRCM_WIDE_DIV", 16));
+    wide_min = (uint32_t)std::max(1, env_int("PBRCM_WIDE_MIN", 1 << 16));
+    if (const char* e = std::getenv("PBRCM_ENGINE"))
+        wide_force = std::string(e) == "wide";
+    wide_ctas = wide_ctas_per_sm() * sms;
     batch_variant = env_int("PBRCM_BATCH_VARIANT", 2);
     if (batch_variant < 0 || batch_variant >= kNumVariants)
         batch_variant = 2;
@@ -158,7 +167,7 @@ Context::~Context()
         cudaSetDevice(device);
     if (stream)
         cudaStreamSynchronize(stream);
-    for (void* p : {(void*)d_pw, (void*)d_rp, (void*)d_ci, (void*)d_node, (void*)d_perm, (void*)d_rec, (void*)d_rec2, (void*)d_stage, (void*)d_hub,
+    for (void* p : {(void*)d_wide, (void*)d_pw, (void*)d_rp, (void*)d_ci, (void*)d_node, (void*)d_perm, (void*)d_rec, (void*)d_rec2, (void*)d_stage, (void*)d_hub,
                     (void*)d_res, (void*)d_gs, (void*)d_agg, (void*)d_jobs, (void*)d_slots, (void*)d_counter, (void*)d_bres,
                     (void*)d_arena})
         if (p)
@@ -203,13 +212,54 @@ bool Context::ensure_single(uint32_t n, uint64_t nnz, bool inputs)
 
 bool Context::ensure_hub(uint64_t nnz) { return grow(d_hub, cap_hub, 4 * (size_t)std::max<uint64_t>(nnz, 1)); }
 
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// The level-synchronous engine: level steps in batches of 8, 16, ... 512,
+// one read of the state between batches.  A matrix that is still running
+// after 1,016 steps (its levels are many, not wide) goes back to the team.
+bool Context::run_wide(const MatrixView& M, const Options& opt, cudaStream_t st)
+{
+    const size_t o_tot = 256, o_inv = o_tot + al256(8 * (size_t)wide_ctas);
+    if (!grow(d_wide, cap_wide, o_inv + 4 * (size_t)M.n))
+        return false;
+    WideState* ws = reinterpret_cast<WideState*>(d_wide);
+    unsigned long long* tot = reinterpret_cast<unsigned long long*>(d_wide + o_tot);
+    if (launch_wide_start(M, opt, ws, sms, st) != cudaSuccess)
+        return false;
+    int total = 0;
+    for (int batch = 8; batch <= 512; batch *= 2) {
+        if (launch_wide_steps(M, opt, ws, tot, wide_ctas, batch, st) != cudaSuccess ||
+            cudaMemcpyAsync(h_aux, &ws->phase, sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return false;
+        total += batch;
+        if (h_aux[0] == kWideDone)
+            break;
+    }
+    if (h_aux[0] != kWideDone) {
+        const uint32_t code = kNeedTeam;
+        return cudaMemcpyAsync(&M.res->status, &code, sizeof(code), cudaMemcpyHostToDevice, st) == cudaSuccess &&
+               cudaStreamSynchronize(st) == cudaSuccess;
+    }
+    if (opt.want_bw && opt.mode == kModeFull &&
+        launch_wide_bandwidth(M, reinterpret_cast<uint32_t*>(d_wide + o_inv), sms, st) != cudaSuccess)
+        return false;
+    return true;
+}
+
 // Runs start search (+ CM + bandwidth) on device buffers already in place.
-// Enqueues on `st`, synchronises, and retries once with hub scratch.
+// Enqueues on `st` and synchronises.  The team engine runs first; it is
+// rerun with hub scratch when a row is longer than its chunks take, and it
+// hands a matrix whose first pass meets a level of at least
+// max(n / wide_div, wide_min) nodes to the level-synchronous engine (rows
+// permitting; that engine hands back the rare matrix it cannot finish).
 int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint64_t nnz, uint32_t* perm,
                             const Options& opt, cudaStream_t st, DevResult* out, float* dev_ms)
 {
     bool with_hub = false;
-    for (int attempt = 0; attempt < 2; ++attempt) {
+    bool try_wide = wide_ctas > 0 && wide_div != 0 && n > 1;
+    bool wide_first = try_wide && wide_force;
+    for (int attempt = 0; attempt < 4; ++attempt) {
         MatrixView M{};
         M.rp = rp;
         M.ci = ci;
@@ -228,13 +278,28 @@ int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
             return PBRCM_ERR_CUDA;
         if (launch_validate(rp, ci, n, (uint32_t)nnz, d_res, sms, st) != cudaSuccess)
             return PBRCM_ERR_CUDA;
-        cudaEventRecord(ev0, st);
-        Options o = opt;
-        apply_team_shape(*this, o);
-        cudaError_t e = launch_team(team_variant, M, o, d_gs, d_agg, team_ctas, st);
+        if (attempt == 0)
+            cudaEventRecord(ev0, st);  // every attempt counts in the device time
+        bool wide_ran = false;
+        if (wide_first) {
+            // the engine needs every row within one chunk: read the valences
+            if (cudaMemcpyAsync(h_res, d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return PBRCM_ERR_CUDA;
+            if (h_res->status == kOk && h_res->maxdeg <= wide_emax()) {
+                if (!run_wide(M, opt, st))
+                    return PBRCM_ERR_CUDA;
+                wide_ran = true;
+            }
+        }
+        if (!wide_ran) {
+            Options o = opt;
+            apply_team_shape(*this, o);
+            o.wide_at = try_wide ? std::max(n / wide_div, wide_min) : 0u;
+            if (launch_team(team_variant, M, o, d_gs, d_agg, team_ctas, st) != cudaSuccess)
+                return PBRCM_ERR_CUDA;
+        }
         cudaEventRecord(ev1, st);
-        if (e != cudaSuccess)
-            return PBRCM_ERR_CUDA;
         if (cudaMemcpyAsync(h_res, d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess)
             return PBRCM_ERR_CUDA;
         if (cudaStreamSynchronize(st) != cudaSuccess)
@@ -242,18 +307,29 @@ int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
         if (dev_ms)
             cudaEventElapsedTime(dev_ms, ev0, ev1);
         *out = *h_res;
+        out->engine = wide_ran ? 1u : 0u;
         if (out->status == kNeedHub && !with_hub) {
             if (!ensure_hub(nnz))
                 return PBRCM_ERR_OOM;
             with_hub = true;
             continue;
         }
+        if (out->status == kNeedWide) {
+            // the team met a wide level: the level-synchronous engine, if
+            // every row fits its chunks, else the team without the hand-over
+            wide_first = out->maxdeg <= wide_emax();
+            try_wide = wide_first;
+            continue;
+        }
+        if (out->status == kNeedTeam) {
+            wide_first = false;
+            try_wide = false;
+            continue;
+        }
         break;
     }
     return PBRCM_OK;
 }
-
-static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // inv (n) | scan partials | mid-row list (n) | long-row list | counters
 size_t Context::permute_work_bytes(uint32_t n, uint64_t nnz)

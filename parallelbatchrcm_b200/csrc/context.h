@@ -25,6 +25,12 @@ struct Context {
     uint32_t barrier = 0;       // team barrier implementation
     uint32_t spec_from = 3;     // speculative split from this search pass on (team-dominated matrices)
     int team_maxc = 0;          // co-resident CTAs of the team kernel
+    // the level-synchronous engine for wide, shallow graphs (wide.cu): a
+    // first-pass level of at least max(n / wide_div, wide_min) nodes hands
+    // the matrix over; wide_force runs it first (rows permitting)
+    uint32_t wide_div = 16, wide_min = 1u << 16;
+    bool wide_force = false;
+    int wide_ctas = 0;  // CTAs per level step (0: engine unavailable)
     // batches: the biggest matrices go to thread-block-cluster teams
     int cluster_size = 2;             // CTAs per cluster (0 or 1: off)
     uint64_t cluster_nnz = 1u << 18;  // matrices with at least this many entries
@@ -53,6 +59,8 @@ struct Context {
     uint32_t* h_aux = nullptr;  // pinned words read back with a result
     GridSync* d_gs = nullptr;
     unsigned long long* d_agg = nullptr;
+    unsigned char* d_wide = nullptr;  // WideState | per-CTA totals | inverse permutation (n)
+    size_t cap_wide = 0;
 
     // matrix permutation workspace (grow only)
     unsigned char* d_pw = nullptr;
@@ -84,6 +92,9 @@ struct Context {
     static size_t connect_work_bytes(uint32_t n);
     int32_t run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint64_t nnz, uint32_t* perm,
                        const Options& opt, cudaStream_t st, DevResult* out, float* dev_ms);
+    // the level-synchronous engine on M (node table, passes, bandwidth);
+    // false on a CUDA error; M.res holds the outcome (kNeedTeam: use the team)
+    bool run_wide(const MatrixView& M, const Options& opt, cudaStream_t st);
 };
 
 int32_t map_status(uint32_t s);

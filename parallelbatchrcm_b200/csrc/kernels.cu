@@ -481,6 +481,16 @@ void launch_perm_inverse(const uint32_t* perm, uint32_t n, uint32_t* inv, DevRes
     k_bw_inverse<<<blocks, 256, 0, st>>>(perm, n, inv, res);
 }
 
+cudaError_t launch_bw_rows(const uint32_t* rp, const uint32_t* ci, uint32_t n, const uint32_t* inv, DevResult* res,
+                           int sms, cudaStream_t st)
+{
+    int blocks = (int)std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)sms * 8);
+    if (blocks < 1)
+        blocks = 1;
+    k_bw_rows<<<blocks, 256, 0, st>>>(rp, ci, n, inv, res);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_bandwidth(const uint32_t* rp, const uint32_t* ci, uint32_t n, const uint32_t* perm, uint32_t* inv,
                              DevResult* res, int sms, cudaStream_t st)
 {

@@ -55,6 +55,8 @@ constexpr size_t kOffNode = (kOffWords + kWordsBytes + 255) & ~(size_t)255;
 constexpr size_t kOffRec = kOffNode + 16 * (size_t)kNoAllocMaxNodes;
 constexpr size_t kScratchBytes = kOffRec + 16 * (size_t)kNoAllocMaxNodes;
 
+static_assert(sizeof(DevResult) <= kOffGs, "DevResult overlaps the GridSync words");
+
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 // The team kernel of kernels.cu, restated for this file's launch: same engine,

@@ -21,7 +21,9 @@ enum : uint32_t {
     kErrDisconnected = 2,
     kErrTimeout = 3,
     kErrCheck = 8,
-    kNeedHub = 100,  // internal: relaunch with hub scratch
+    kNeedHub = 100,   // internal: relaunch with hub scratch
+    kNeedWide = 101,  // internal: the first pass met a wide level; run the level-synchronous engine
+    kNeedTeam = 102,  // internal: the level-synchronous engine cannot take this matrix; run the team
 };
 
 // One record per queue position: node, row start, valence, edge id base.
@@ -63,6 +65,8 @@ struct alignas(16) DevResult {
     uint32_t levels;
     uint32_t placed;
     uint32_t maxdeg;   // largest valence (written by the validation kernel)
+    uint32_t engine;   // set by the host: 0 team engine, 1 level-synchronous engine
+    uint32_t pad_;
     unsigned long long bandwidth;      // max |inv[i]-inv[j]|
     unsigned long long initial_bw;
     unsigned long long profile_lo;     // sum inv[i] - min(inv[row])   (CM order)
@@ -133,6 +137,23 @@ struct Options {
     uint32_t solo_parents;  // ... and at most this many parents
     uint32_t barrier;       // team barrier: 0 counter, 1 flag array
     uint32_t spec_from;     // speculative split from this search pass on (0: only for solo-dominated matrices)
+    uint32_t wide_at;       // first BFS pass: a level of at least this many nodes hands the matrix to the
+                            // level-synchronous engine (kNeedWide; 0 = never)
+};
+
+// State of the level-synchronous engine (wide.cu), one per matrix in device
+// memory: the level being expanded and the start-search bookkeeping, advanced
+// by one kernel after every level.
+enum : uint32_t { kWideSearch = 0, kWideFinal = 1, kWideDone = 2 };
+struct alignas(16) WideState {
+    uint32_t a, b, Ka, Kb;       // frontier positions [a, b), its edge ids [Ka, Kb)
+    uint32_t L, last_start;      // level index in the pass, first position of the newest level
+    uint32_t phase;              // kWideSearch / kWideFinal / kWideDone
+    uint32_t base;               // key base of the pass
+    uint32_t start, passes, ecc, lastdist;
+    uint32_t pid;                // pass number in the claim key space
+    uint32_t steps;              // level steps run (bounded by the host)
+    uint32_t pad[2];
 };
 
 constexpr uint32_t kModeFull = 0;
