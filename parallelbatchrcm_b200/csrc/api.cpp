@@ -140,9 +140,11 @@ int32_t Context::init(int dev)
     // wide, shallow graphs: PBRCM_WIDE_DIV (0: never), PBRCM_WIDE_MIN,
     // PBRCM_ENGINE=wide to run the level-synchronous engine first
     wide_div = (uint32_t)std::max(0, env_int("PBRCM_WIDE_DIV", 16));
-    wide_min = (uint32_t)std::max(1, env_int("PBRCM_WIDE_MIN", 1 << 16));
+    wide_min = (uint32_t)std::max(1, env_int("PBRCM_WIDE_MIN", 1 << 18));
     if (const char* e = std::getenv("PBRCM_ENGINE"))
         wide_force = std::string(e) == "wide";
+    wide_fused = env_int("PBRCM_WIDE_FUSED", 1) != 0;
+    wide_batch_pass = env_int("PBRCM_WIDE_BATCH_PASS", 1) != 0;
     wide_ctas = wide_ctas_per_sm() * sms;
     batch_variant = env_int("PBRCM_BATCH_VARIANT", 2);
     if (batch_variant < 0 || batch_variant >= kNumVariants)
@@ -214,9 +216,14 @@ bool Context::ensure_hub(uint64_t nnz) { return grow(d_hub, cap_hub, 4 * (size_t
 
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// The level-synchronous engine: level steps in batches of 8, 16, ... 512,
-// one read of the state between batches.  A matrix that is still running
-// after 1,016 steps (its levels are many, not wide) goes back to the team.
+// The level-synchronous engine: level steps in batches, one read of the
+// state between batches.  While no pass has finished the batches grow 8, 16,
+// 32, ...; after that a batch is the rest of a pass as long as the last one
+// (the final pass, from the same start as the last search pass, has exactly
+// its levels).  A matrix still running after kWideMaxSteps steps (its levels
+// are many, not wide) goes back to the team.
+static constexpr int kWideMaxSteps = 1024;
+
 bool Context::run_wide(const MatrixView& M, const Options& opt, cudaStream_t st)
 {
     const size_t o_tot = 256, o_inv = o_tot + al256(8 * (size_t)wide_ctas);
@@ -224,19 +231,30 @@ bool Context::run_wide(const MatrixView& M, const Options& opt, cudaStream_t st)
         return false;
     WideState* ws = reinterpret_cast<WideState*>(d_wide);
     unsigned long long* tot = reinterpret_cast<unsigned long long*>(d_wide + o_tot);
-    if (launch_wide_start(M, opt, ws, sms, st) != cudaSuccess)
+    if (cudaMemsetAsync(ws, 0, sizeof(WideState), st) != cudaSuccess ||
+        launch_wide_start(M, opt, ws, sms, st) != cudaSuccess)
         return false;
-    int total = 0;
-    for (int batch = 8; batch <= 512; batch *= 2) {
-        if (launch_wide_steps(M, opt, ws, tot, wide_ctas, batch, st) != cudaSuccess ||
-            cudaMemcpyAsync(h_aux, &ws->phase, sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    WideState* hs = reinterpret_cast<WideState*>(h_aux);
+    static_assert(sizeof(WideState) <= 64, "the state is read back through the 64-byte pinned words");
+    int total = 0, grow_batch = 8;
+    bool done = false;
+    while (total < kWideMaxSteps) {
+        int batch = grow_batch;
+        if (wide_batch_pass && total > 0 && hs->prev_levels > 0)
+            batch = std::max(2, (int)hs->prev_levels + 1 - (int)hs->L);
+        batch = std::min(batch, kWideMaxSteps - total);
+        if (launch_wide_steps(M, opt, ws, tot, wide_ctas, batch, wide_fused, st) != cudaSuccess ||
+            cudaMemcpyAsync(hs, ws, sizeof(WideState), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess)
             return false;
         total += batch;
-        if (h_aux[0] == kWideDone)
+        grow_batch *= 2;
+        if (hs->phase == kWideDone) {
+            done = true;
             break;
+        }
     }
-    if (h_aux[0] != kWideDone) {
+    if (!done) {
         const uint32_t code = kNeedTeam;
         return cudaMemcpyAsync(&M.res->status, &code, sizeof(code), cudaMemcpyHostToDevice, st) == cudaSuccess &&
                cudaStreamSynchronize(st) == cudaSuccess;

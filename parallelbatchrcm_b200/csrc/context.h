@@ -28,8 +28,10 @@ struct Context {
     // the level-synchronous engine for wide, shallow graphs (wide.cu): a
     // first-pass level of at least max(n / wide_div, wide_min) nodes hands
     // the matrix over; wide_force runs it first (rows permitting)
-    uint32_t wide_div = 16, wide_min = 1u << 16;
+    uint32_t wide_div = 16, wide_min = 1u << 18;
     bool wide_force = false;
+    bool wide_fused = true;        // the place kernel's last CTA advances the level state
+    bool wide_batch_pass = true;   // batches sized by the last pass's levels (else 8, 16, 32, ...)
     int wide_ctas = 0;  // CTAs per level step (0: engine unavailable)
     // batches: the biggest matrices go to thread-block-cluster teams
     int cluster_size = 2;             // CTAs per cluster (0 or 1: off)

@@ -1235,7 +1235,7 @@ template <int B, int EMAX, class TeamT>
 __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, unsigned long long* agg,
                          uint32_t& step, const Options& opt, uint32_t start, uint32_t base, bool sorted,
                          bool write_perm, bool reverse, uint32_t& placed, uint32_t& nlevels, uint32_t& last_start,
-                         uint32_t& wide_f, uint32_t& wide_e, uint32_t wide_at)
+                         uint32_t& wide_f, uint32_t& wide_e)
 {
     Chunk<B, EMAX> ch{s, M, base};
     const uint32_t t = threadIdx.x;
@@ -1414,9 +1414,10 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, uns
             return false;
         const uint32_t tot_cnt = (uint32_t)(all & 0xFFFFFFFFull);
         const uint32_t tot_esum = (uint32_t)(all >> 32);
-        if (wide_at != 0 && tot_cnt >= wide_at) {
-            // a level this wide: the level-synchronous engine takes the
-            // matrix (every CTA has the same totals and leaves here)
+        if (opt.wide_at != 0 && tot_cnt >= opt.wide_at && base == 2u * M.nnz + 3u) {
+            // a level this wide in the first pass (key base of pass 1): the
+            // level-synchronous engine takes the matrix (every CTA has the
+            // same totals and leaves here)
             if (R == 0 && t == 0)
                 set_status(M.res, kNeedWide, 0);
             return false;
@@ -1583,7 +1584,6 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& tea
         start = n / 2;
     }
     uint32_t lastdist = 0;
-    bool first_bfs = true;  // the first pass may hand a wide matrix over (opt.wide_at)
     while (true) {
         if (!searching && opt.mode == kModeStartOnly)
             break;
@@ -1610,9 +1610,8 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& tea
         const uint32_t step0 = step;
         uint32_t pl = 0, nl = 0, ls = 0, wf = 0, we = 0;
         if (!bfs_pass<B, EMAX>(s, spec_half ? M2 : M, tm, ag, stp, opt, start, base, ordered, ordered,
-                               ordered && opt.reverse != 0, pl, nl, ls, wf, we, first_bfs ? opt.wide_at : 0u))
+                               ordered && opt.reverse != 0, pl, nl, ls, wf, we))
             return;
-        first_bfs = false;
         if (!searching) {
             placed = pl;
             nlevels = nl;

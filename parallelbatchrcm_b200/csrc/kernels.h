@@ -79,7 +79,9 @@ cudaError_t launch_bw_rows(const uint32_t* rp, const uint32_t* ci, uint32_t n, c
                            int sms, cudaStream_t st);
 // The level-synchronous engine (wide.cu).  launch_wide_start fills the node
 // table and starts the first pass; launch_wide_steps enqueues `steps` level
-// steps (each a no-op once ws->phase is kWideDone); launch_wide_bandwidth
+// steps (each a no-op once ws->phase is kWideDone; fused: the place
+// kernel's last CTA advances the state, else a one-CTA kernel after it);
+// launch_wide_bandwidth
 // writes the bandwidth and profiles of the result (inv: n words).  `ctas` CTAs
 // per step (wide_ctas_per_sm() x SMs fills the GPU once); rows must be at
 // most wide_emax() long.
@@ -87,7 +89,7 @@ int wide_ctas_per_sm();
 uint32_t wide_emax();
 cudaError_t launch_wide_start(const MatrixView& M, const Options& opt, WideState* ws, int sms, cudaStream_t st);
 cudaError_t launch_wide_steps(const MatrixView& M, const Options& opt, WideState* ws, unsigned long long* tot,
-                              int ctas, int steps, cudaStream_t st);
+                              int ctas, int steps, bool fused, cudaStream_t st);
 cudaError_t launch_wide_bandwidth(const MatrixView& M, uint32_t* inv, int sms, cudaStream_t st);
 
 }  // namespace pbrcm

@@ -137,8 +137,8 @@ struct Options {
     uint32_t solo_parents;  // ... and at most this many parents
     uint32_t barrier;       // team barrier: 0 counter, 1 flag array
     uint32_t spec_from;     // speculative split from this search pass on (0: only for solo-dominated matrices)
-    uint32_t wide_at;       // first BFS pass: a level of at least this many nodes hands the matrix to the
-                            // level-synchronous engine (kNeedWide; 0 = never)
+    uint32_t wide_at;       // first BFS pass (key base 2 nnz + 3): a level of at least this many nodes
+                            // hands the matrix to the level-synchronous engine (kNeedWide; 0 = never)
 };
 
 // State of the level-synchronous engine (wide.cu), one per matrix in device
@@ -153,7 +153,8 @@ struct alignas(16) WideState {
     uint32_t start, passes, ecc, lastdist;
     uint32_t pid;                // pass number in the claim key space
     uint32_t steps;              // level steps run (bounded by the host)
-    uint32_t pad[2];
+    uint32_t ticket;             // CTAs of the place kernel done with this step
+    uint32_t prev_levels;        // levels of the last finished pass (the host sizes its batches by it)
 };
 
 constexpr uint32_t kModeFull = 0;

@@ -15,13 +15,15 @@
 //                   its run's level-relative edge offset; per-CTA totals;
 //   k_wide_place    the same runs: prefix of the totals, then the staged
 //                   children placed (records, permutation) and their edges
-//                   claimed for the next level (Chunk::place_staged);
-//   k_wide_advance  one CTA: the next level, or at the end of a pass the
-//                   start search's next step (simple_peripheral.cpp:92-141,
-//                   as reorder_matrix runs it) and the next pass's start.
-// The host enqueues level steps in growing batches and reads the state only
-// between batches; steps after the end return at once.  Every result (start,
-// passes, levels, permutation, bandwidth) is the team engine's.
+//                   claimed for the next level (Chunk::place_staged); the
+//                   last CTA to finish advances the state: the next level,
+//                   or at the end of a pass the start search's next step
+//                   (simple_peripheral.cpp:92-141, as reorder_matrix runs
+//                   it) and the next pass's start.
+// The host enqueues level steps in batches sized by the previous pass's
+// level count and reads the state only between batches; steps after the end
+// return at once.  Every result (start, passes, levels, permutation,
+// bandwidth) is the team engine's.
 #include <algorithm>
 #include <cstdint>
 
@@ -94,34 +96,6 @@ __global__ void __launch_bounds__(B) k_wide_collect(MatrixView M, const WideStat
     }
     if (threadIdx.x == 0)
         tot[blockIdx.x] = (unsigned long long)cnt | ((unsigned long long)esum << 32);
-}
-
-template <int B, int EMAX>
-__global__ void __launch_bounds__(B) k_wide_place(MatrixView M, const WideState* ws, const unsigned long long* tot,
-                                                  uint32_t reverse)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto& s = *reinterpret_cast<Smem<B, EMAX>*>(smem_raw);
-    const WideState st = load_state(ws);
-    if (st.phase == kWideDone || read_status(M.res) != 0)
-        return;
-    const uint32_t R = blockIdx.x;
-    unsigned long long pc = 0, pe = 0;
-    for (uint32_t r = threadIdx.x; r < R; r += B) {
-        const unsigned long long u = __ldcg(tot + r);
-        pc += u & 0xFFFFFFFFull;
-        pe += u >> 32;
-    }
-    block_reduce_sum2<B>(pc, pe, s.tmp64);
-    const uint32_t cnt = (uint32_t)(__ldcg(tot + R) & 0xFFFFFFFFull);
-    if (cnt == 0)
-        return;
-    uint32_t p0, p1;
-    cta_run(st, R, gridDim.x, p0, p1);
-    const uint32_t stage_base = __ldcg(&reinterpret_cast<const uint4*>(M.rec)[p0].w) - st.Ka;
-    Chunk<B, EMAX> ch{s, M, st.base};
-    ch.place_staged(stage_base, cnt, st.b + (uint32_t)pc, st.Kb + (uint32_t)pe, st.phase == kWideFinal,
-                    reverse != 0);
 }
 
 // Starts a pass from st.start: key base, level 0 = the start node, its edges
@@ -209,16 +183,13 @@ __global__ void __launch_bounds__(B) k_wide_init(MatrixView M)
     init_nodes<B>(M, blockIdx.x, gridDim.x);
 }
 
-// After a level step: the next level, or the end of a pass.  One CTA.
+// After a level step: the next level, or the end of a pass.  Block-wide, by
+// the last CTA of the place kernel (every other CTA of the step is done).
 template <int B>
-__global__ void __launch_bounds__(B) k_wide_advance(MatrixView M, WideState* ws, const unsigned long long* tot,
-                                                    uint32_t G, Options opt)
+__device__ void wide_advance(const MatrixView& M, WideState* ws, const unsigned long long* tot, uint32_t G,
+                             const Options& opt, unsigned long long* tmp, uint32_t* bcast)
 {
-    __shared__ unsigned long long tmp[2 * (B / 32) + 2];
-    __shared__ uint32_t s_next;
     WideState st = load_state(ws);
-    if (st.phase == kWideDone)
-        return;
     const uint32_t t = threadIdx.x;
     const uint32_t n = M.n;
     if (read_status(M.res) != 0) {
@@ -251,6 +222,8 @@ __global__ void __launch_bounds__(B) k_wide_advance(MatrixView M, WideState* ws,
     }
     // the pass has ended: placed st.b nodes in st.L + 1 levels
     const uint32_t placed = st.b, nl = st.L + 1, ls = st.last_start;
+    if (t == 0)
+        __stcg(&ws->prev_levels, nl);
     if (st.phase == kWideFinal) {
         if (t == 0) {
             if (placed != n) {
@@ -286,9 +259,9 @@ __global__ void __launch_bounds__(B) k_wide_advance(MatrixView M, WideState* ws,
             }
         } else {
             if (t == 0)
-                s_next = next_peripheral_start(M, opt.outnodes, ls);
+                bcast[0] = next_peripheral_start(M, opt.outnodes, ls);
             __syncthreads();
-            st.start = s_next;
+            st.start = bcast[0];
             st.lastdist = dist;
             st.passes += 1;
             if (st.passes > n + 1) {  // eccentricities only grow; cannot happen on a valid run
@@ -302,6 +275,62 @@ __global__ void __launch_bounds__(B) k_wide_advance(MatrixView M, WideState* ws,
     __syncthreads();
     if (t == 0)
         store_state(ws, st);
+}
+
+template <int B, int EMAX>
+__global__ void __launch_bounds__(B) k_wide_place(MatrixView M, WideState* ws, const unsigned long long* tot,
+                                                  Options opt, uint32_t fused)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto& s = *reinterpret_cast<Smem<B, EMAX>*>(smem_raw);
+    const WideState st = load_state(ws);
+    if (st.phase == kWideDone)
+        return;  // every CTA reads the same phase
+    const uint32_t R = blockIdx.x, G = gridDim.x;
+    if (read_status(M.res) == 0) {
+        unsigned long long pc = 0, pe = 0;
+        for (uint32_t r = threadIdx.x; r < R; r += B) {
+            const unsigned long long u = __ldcg(tot + r);
+            pc += u & 0xFFFFFFFFull;
+            pe += u >> 32;
+        }
+        block_reduce_sum2<B>(pc, pe, s.tmp64);
+        const uint32_t cnt = (uint32_t)(__ldcg(tot + R) & 0xFFFFFFFFull);
+        if (cnt > 0) {
+            uint32_t p0, p1;
+            cta_run(st, R, G, p0, p1);
+            const uint32_t stage_base = __ldcg(&reinterpret_cast<const uint4*>(M.rec)[p0].w) - st.Ka;
+            Chunk<B, EMAX> ch{s, M, st.base};
+            ch.place_staged(stage_base, cnt, st.b + (uint32_t)pc, st.Kb + (uint32_t)pe, st.phase == kWideFinal,
+                            opt.reverse != 0);
+        }
+    }
+    if (!fused)
+        return;  // k_wide_advance follows
+    // the last CTA to finish advances the state
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s.bcast[1] = atomicAdd(&ws->ticket, 1u) == G - 1 ? 1u : 0u;
+    }
+    __syncthreads();
+    if (s.bcast[1] == 0)
+        return;
+    __threadfence();
+    if (threadIdx.x == 0)
+        ws->ticket = 0;
+    wide_advance<B>(M, ws, tot, G, opt, s.tmp64, s.bcast);
+}
+
+template <int B>
+__global__ void __launch_bounds__(B) k_wide_advance(MatrixView M, WideState* ws, const unsigned long long* tot,
+                                                    uint32_t G, Options opt)
+{
+    __shared__ unsigned long long tmp[2 * (B / 32) + 2];
+    __shared__ uint32_t bcast[1];
+    if (load_state(ws).phase == kWideDone)
+        return;
+    wide_advance<B>(M, ws, tot, G, opt, tmp, bcast);
 }
 
 // inv[rec[pos].node] = pos (Cuthill-McKee positions) for the bandwidth rows.
@@ -351,13 +380,14 @@ cudaError_t launch_wide_start(const MatrixView& M, const Options& opt, WideState
 }
 
 cudaError_t launch_wide_steps(const MatrixView& M, const Options& opt, WideState* ws, unsigned long long* tot,
-                              int ctas, int steps, cudaStream_t st)
+                              int ctas, int steps, bool fused, cudaStream_t st)
 {
     const size_t smem = sizeof(Smem<kWideB, kWideEmax>);
     for (int i = 0; i < steps; ++i) {
         k_wide_collect<kWideB, kWideEmax><<<ctas, kWideB, smem, st>>>(M, ws, tot);
-        k_wide_place<kWideB, kWideEmax><<<ctas, kWideB, smem, st>>>(M, ws, tot, opt.reverse);
-        k_wide_advance<kWideB><<<1, kWideB, 0, st>>>(M, ws, tot, (uint32_t)ctas, opt);
+        k_wide_place<kWideB, kWideEmax><<<ctas, kWideB, smem, st>>>(M, ws, tot, opt, fused ? 1u : 0u);
+        if (!fused)
+            k_wide_advance<kWideB><<<1, kWideB, 0, st>>>(M, ws, tot, (uint32_t)ctas, opt);
     }
     return cudaGetLastError();
 }
