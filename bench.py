@@ -22,8 +22,8 @@ workload (rank 0; other ranks exit 0).  Under torchrun each rank runs an
 independent replica (the single-matrix path does not shard); value is the
 sum over ranks of reorders / the max over ranks of the timed time.
 
---workload batch|serve|permute|connect run the many-matrix, serving, P A P^T
-and connectivity-repair benchmarks instead
+--workload batch|serve|permute|connect|wide run the many-matrix, serving,
+P A P^T, connectivity-repair and wide-graph benchmarks instead
 (see parallelbatchrcm_b200/workloads.py).
 """
 from __future__ import annotations
@@ -334,7 +334,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "permute", "connect"])
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "permute", "connect", "wide"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_init()

@@ -25,7 +25,7 @@ from dataclasses import dataclass
 import numpy as np
 
 __all__ = [
-    "Csr", "grid2d", "grid3d", "rgg", "from_edges", "connect_components",
+    "Csr", "grid2d", "grid3d", "rgg", "erdos_renyi", "from_edges", "connect_components",
     "write_mtx", "mixed_batch_specs", "make_from_spec", "poisson_stream_specs",
 ]
 
@@ -175,6 +175,17 @@ def rgg(n: int, kmin: int = 6, kmax: int = 14, long_frac: float = 0.001, seed: i
         m = connect_components(m)
     m.name = f"rgg_{n}_k{kmin}-{kmax}_s{seed}" + ("" if connect else "_raw")
     return m
+
+
+def erdos_renyi(n: int, deg: int, seed: int = 2) -> Csr:
+    """Random graph: n * deg / 2 uniformly random node pairs (self pairs and
+    repeats merge), symmetrised, joined by the loader's rule.  Its BFS levels
+    are few and wide (2M nodes, degree 14: 10 levels, the widest 1.46M)."""
+    rng = np.random.default_rng(seed)
+    m = n * deg // 2
+    g = connect_components(from_edges(n, rng.integers(0, n, m), rng.integers(0, n, m)))
+    g.name = f"er_{n}_d{deg}_s{seed}"
+    return g
 
 
 def write_mtx(m: Csr, path: str, symmetric: bool = True, field: str = "real") -> None:

@@ -453,7 +453,88 @@ def run_connect(args, ws, rank, local):
     return 0
 
 
+def run_wide(args, ws, rank, local):
+    """Full reorder of a 2M-node random graph of degree 14 (10 BFS levels, the
+    widest 1.46M nodes) through pbrcm_reorder_device, device-resident, L2
+    flushed between steps: the default context (the team kernel hands the
+    matrix to the level-synchronous engine) beside a team-only context
+    (PBRCM_WIDE_DIV=0).  cpu_baseline: the oracle's serial restatement of the
+    reference's findPeripheral + rcm_seq<true>, one full reorder."""
+    import torch
+
+    import parallelbatchrcm_b200 as P
+    from parallelbatchrcm_b200 import gen
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    m = gen.erdos_renyi(2_000_000, 14, seed=2)
+    n, nnz = m.n, m.nnz
+    ctx = P.Context(local)
+    old = os.environ.get("PBRCM_WIDE_DIV")
+    os.environ["PBRCM_WIDE_DIV"] = "0"
+    try:
+        team_ctx = P.Context(local)
+    finally:
+        if old is None:
+            os.environ.pop("PBRCM_WIDE_DIV", None)
+        else:
+            os.environ["PBRCM_WIDE_DIV"] = old
+    stream = torch.cuda.Stream(device=dev)
+    rp = torch.from_numpy(m.row_ptr.view(np.int32)).to(dev)
+    ci = torch.from_numpy(m.col_idx.view(np.int32)).to(dev)
+    perm = torch.empty(n, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=dev)
+
+    def step(c):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, res = P.reorder_device(rp, ci, perm, reverse=True, ctx=c, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), res
+
+    for _ in range(max(3, args.warmup)):
+        step(ctx)
+        step(team_ctx)
+    ms, ms_team = [], []
+    for _ in range(args.steps):
+        t, res = step(ctx)
+        ms.append(t)
+        ms_team.append(step(team_ctx)[0])
+    p_auto = perm.cpu().numpy().copy()
+    step(team_ctx)
+    same = bool(np.array_equal(p_auto, perm.cpu().numpy()))
+    ms_med, team_med = statistics.median(ms), statistics.median(ms_team)
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+        import oracle as O
+        t0 = time.perf_counter()
+        O.full_reorder(m.row_ptr, m.col_idx, reverse=True)
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": 1.0 / cpu_s, "unit": "reorders/s", "cores": 1, "kind": "port",
+               "sample": "1 full reorder of the same graph with the C oracle (serial)"}
+    line = {
+        "metric": "reorders/s (full reorder: start search + RCM + bandwidth)", "value": 1e3 / ms_med,
+        "unit": "reorders/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_med,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded random graph, degree 14)",
+        "config": {"workload": "erdos_renyi_2M_d14_rcm", "n": n, "nnz": nnz, "reverse": True, "start": "auto",
+                   "l2": "flushed (256 MiB write) between steps"},
+        "engine": res["engine"], "levels": res["levels"], "passes": res["peripheral_passes"],
+        "team_only": {"value": 1e3 / team_med, "unit": "reorders/s", "ms_per_step": team_med,
+                      "same_permutation": same},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(args, ws, rank, local):
+    if args.workload == "wide":
+        return run_wide(args, ws, rank, local)
     if args.workload == "connect":
         return run_connect(args, ws, rank, local)
     if args.workload == "permute":
