@@ -1414,10 +1414,12 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, uns
             return false;
         const uint32_t tot_cnt = (uint32_t)(all & 0xFFFFFFFFull);
         const uint32_t tot_esum = (uint32_t)(all >> 32);
-        if (opt.wide_at != 0 && tot_cnt >= opt.wide_at && base == 2u * M.nnz + 3u) {
-            // a level this wide in the first pass (key base of pass 1): the
-            // level-synchronous engine takes the matrix (every CTA has the
-            // same totals and leaves here)
+        if (opt.wide_at != 0 && tot_cnt >= opt.wide_at && base == 2u * M.nnz + 3u && M.cf == 0 &&
+            G == gridDim.x) {
+            // a level this wide in the first pass of the whole team (key base
+            // of pass 1 in the main claim word; never a half team, whose
+            // other half would wait for it): the level-synchronous engine
+            // takes the matrix (every CTA has the same totals and leaves)
             if (R == 0 && t == 0)
                 set_status(M.res, kNeedWide, 0);
             return false;
