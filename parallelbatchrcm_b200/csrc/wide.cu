@@ -15,7 +15,7 @@
 //                   its run's level-relative edge offset; per-CTA totals;
 //   k_wide_place    the same runs: prefix of the totals, then the staged
 //                   children placed (records, permutation) and their edges
-//                   claimed for the next level (Chunk::place_staged); the
+//                   claimed for the next level, 16 lanes per child; the
 //                   last CTA to finish advances the state: the next level,
 //                   or at the end of a pass the start search's next step
 //                   (simple_peripheral.cpp:92-141, as reorder_matrix runs
@@ -277,6 +277,38 @@ __device__ void wide_advance(const MatrixView& M, WideState* ws, const unsigned 
         store_state(ws, st);
 }
 
+// Places the `count` children staged at M.stage[at..] at positions P0.. with
+// edge ids K0 + their staged edge offsets, and claims their edges: what
+// Chunk::place_staged computes, with 16 lanes per child so that a row is read
+// by consecutive lanes and each child's record is one broadcast load.
+template <int B>
+__device__ void wide_place_children(const MatrixView& M, uint32_t base, uint32_t at, uint32_t count, uint32_t P0,
+                                    uint32_t K0, bool write_perm, bool reverse)
+{
+    constexpr uint32_t kLanes = 16;
+    const uint32_t sub = threadIdx.x & (kLanes - 1);
+    for (uint32_t i = threadIdx.x / kLanes; i < count; i += B / kLanes) {
+        uint4 r = make_uint4(0u, 0u, 0u, 0u);
+        if (PB_CHECK(M.res, (uint64_t)at + i < M.nnz, 146))
+            r = __ldcg(reinterpret_cast<const uint4*>(M.stage) + at + i);
+        const uint32_t pos = P0 + i;
+        const uint32_t eb = K0 + r.w;
+        if (sub == 0 && PB_CHECK(M.res, pos < M.n, 147)) {
+            __stcg(reinterpret_cast<uint4*>(M.rec) + pos, make_uint4(r.x, r.y, r.z, eb));
+            if (write_perm)
+                M.perm[reverse ? M.n - 1 - pos : pos] = r.x;
+        }
+        const uint32_t kb = base - 1u - eb;
+        for (uint32_t k = sub; k < r.z; k += kLanes) {
+            if (PB_CHECK(M.res, (uint64_t)r.y + k < M.nnz, 148)) {
+                const uint32_t d = ld_ro(M.ci + r.y + k);
+                if (PB_CHECK(M.res, d < M.n, 149))
+                    atomicMax(claim_ptr(M, d), kb - k);
+            }
+        }
+    }
+}
+
 template <int B, int EMAX>
 __global__ void __launch_bounds__(B) k_wide_place(MatrixView M, WideState* ws, const unsigned long long* tot,
                                                   Options opt, uint32_t fused)
@@ -300,9 +332,8 @@ __global__ void __launch_bounds__(B) k_wide_place(MatrixView M, WideState* ws, c
             uint32_t p0, p1;
             cta_run(st, R, G, p0, p1);
             const uint32_t stage_base = __ldcg(&reinterpret_cast<const uint4*>(M.rec)[p0].w) - st.Ka;
-            Chunk<B, EMAX> ch{s, M, st.base};
-            ch.place_staged(stage_base, cnt, st.b + (uint32_t)pc, st.Kb + (uint32_t)pe, st.phase == kWideFinal,
-                            opt.reverse != 0);
+            wide_place_children<B>(M, st.base, stage_base, cnt, st.b + (uint32_t)pc, st.Kb + (uint32_t)pe,
+                                   st.phase == kWideFinal, opt.reverse != 0);
         }
     }
     if (!fused)
