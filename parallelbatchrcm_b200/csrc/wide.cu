@@ -309,12 +309,16 @@ __device__ void wide_place_children(const MatrixView& M, uint32_t base, uint32_t
     }
 }
 
-template <int B, int EMAX>
+// B threads per CTA, the same number of CTAs as the collect (the CTAs' runs
+// match); no chunk buffers, so B can be twice the collect's threads.
+template <int B>
 __global__ void __launch_bounds__(B) k_wide_place(MatrixView M, WideState* ws, const unsigned long long* tot,
                                                   Options opt, uint32_t fused)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto& s = *reinterpret_cast<Smem<B, EMAX>*>(smem_raw);
+    __shared__ struct {
+        unsigned long long tmp64[2 * (B / 32) + 2];
+        uint32_t bcast[2];
+    } s;
     const WideState st = load_state(ws);
     if (st.phase == kWideDone)
         return;  // every CTA reads the same phase
@@ -379,6 +383,7 @@ __global__ void __launch_bounds__(256) k_wide_inverse(MatrixView M, uint32_t* in
 
 namespace {
 constexpr int kWideB = 256, kWideEmax = 1024;
+constexpr int kPlaceB = 512;  // threads of the place kernel's CTAs
 }
 
 int wide_ctas_per_sm()
@@ -386,17 +391,14 @@ int wide_ctas_per_sm()
     int occ = 0;
     const size_t smem = sizeof(Smem<kWideB, kWideEmax>);
     if (cudaFuncSetAttribute(k_wide_collect<kWideB, kWideEmax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess ||
-        cudaFuncSetAttribute(k_wide_place<kWideB, kWideEmax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
         return 0;
-    int occ2 = 0;
+    // the place kernel needs no co-residency (its last CTA takes a ticket),
+    // so the collect's occupancy alone sets the number of CTAs
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_wide_collect<kWideB, kWideEmax>, kWideB, smem) !=
-            cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_wide_place<kWideB, kWideEmax>, kWideB, smem) !=
-            cudaSuccess)
+        cudaSuccess)
         return 0;
-    return std::max(1, std::min(occ, occ2));
+    return std::max(1, occ);
 }
 
 uint32_t wide_emax() { return (uint32_t)kWideEmax; }
@@ -416,7 +418,7 @@ cudaError_t launch_wide_steps(const MatrixView& M, const Options& opt, WideState
     const size_t smem = sizeof(Smem<kWideB, kWideEmax>);
     for (int i = 0; i < steps; ++i) {
         k_wide_collect<kWideB, kWideEmax><<<ctas, kWideB, smem, st>>>(M, ws, tot);
-        k_wide_place<kWideB, kWideEmax><<<ctas, kWideB, smem, st>>>(M, ws, tot, opt, fused ? 1u : 0u);
+        k_wide_place<kPlaceB><<<ctas, kPlaceB, 0, st>>>(M, ws, tot, opt, fused ? 1u : 0u);
         if (!fused)
             k_wide_advance<kWideB><<<1, kWideB, 0, st>>>(M, ws, tot, (uint32_t)ctas, opt);
     }
