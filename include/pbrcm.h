@@ -187,10 +187,14 @@ typedef struct pbrcm_matrix {
 
 /*
  * Reorders `count` independent matrices (HOST buffers) with one persistent
- * launch: the CSRs are packed into one device arena, small matrices run one
- * CTA each, matrices above the autotuned cutoff run on cooperative teams.
- * results[i] receives matrix i's result.  The reference has no batched form;
- * each permutation equals the single-matrix result.
+ * launch: the CSRs are packed into one device arena and copied in waves
+ * while the kernel already reorders the ones that have arrived; every CTA
+ * runs several thread groups, one matrix each, and the biggest matrices run
+ * on thread-block-cluster teams (the shape is the context's tuning: see
+ * pbrcm_autotune).  results[i] receives matrix i's result; its device_ms is
+ * the time from the batch's first matrix taken to matrix i's result.  The
+ * reference has no batched form; each permutation equals the single-matrix
+ * result.
  */
 PBRCM_API int32_t pbrcm_reorder_batch(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t count,
                             const pbrcm_options* opts, pbrcm_result* results);
@@ -199,6 +203,57 @@ PBRCM_API int32_t pbrcm_reorder_batch(pbrcm_context* ctx, const pbrcm_matrix* ma
  * are device pointers; `mats` itself is a host array). */
 PBRCM_API int32_t pbrcm_reorder_batch_device(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t count,
                                    const pbrcm_options* opts, pbrcm_result* results, void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* Autotuner of the batch and serving shapes.                              */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * The shape settings of the batched and serving paths.  They replace the
+ * reference's compile-time constants (include/rcm_gpu_batch_params.h:36-46:
+ * BlockSizePow, MaxElementsPerThreadPow, QueueSize, Overalloc), which set
+ * one batch shape for every input; here they are measured per device.
+ */
+typedef struct pbrcm_tuning {
+    uint32_t batch_pool;       /* thread groups per 512-thread CTA of the batch kernel:
+                                  0 = 1 x 512 threads, 1 = 2 x 256, 2 = 4 x 128, 3 = 8 x 64 */
+    uint32_t cluster_size;     /* CTAs of a cluster team for the biggest matrices (1 = none) */
+    uint32_t cluster_max;      /* at most this many matrices of a batch get a cluster team */
+    uint32_t cluster_nnz;      /* ... and only those with at least this many entries */
+    uint32_t session_cutoff_n; /* serving: requests with more nodes run on a cooperative team */
+    uint32_t session_pool;     /* serving: CTA shape of the other requests (0 = 512 threads,
+                                  4 = 128 threads, four per SM) */
+    uint32_t sms;              /* streaming multiprocessors of the device it was measured on */
+    uint32_t trials;           /* settings measured */
+    uint32_t source;           /* 0 built-in defaults, 1 a tuning file, 2 measured or set */
+    float default_ms;          /* calibration batch with the settings the tuner started from */
+    float best_ms;             /* ... with the chosen settings */
+    float session_default_ms;  /* calibration serving replay: makespan before / after */
+    float session_best_ms;
+} pbrcm_tuning;
+
+/*
+ * Measures the batch shapes on `mats` (a calibration batch on HOST buffers,
+ * e.g. a sample of the caller's own workload): the thread-group shape, the
+ * cluster-team size, count and threshold, then the serving cutoff (a replay
+ * of the batch through a session), each against the current best.  Every
+ * setting tried must give bit-identical permutations (it returns
+ * PBRCM_ERR_CHECK otherwise).  The chosen settings become the context's;
+ * with cache_path they are also written there, keyed by the device's SM
+ * count and the library version, for pbrcm_tuning_load or the PBRCM_TUNING
+ * environment variable (read by pbrcm_context_create; the PBRCM_* knobs
+ * still override single settings).  `out` (nullable) receives them.
+ */
+PBRCM_API int32_t pbrcm_autotune(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t count,
+                                 const pbrcm_options* opts, const char* cache_path, pbrcm_tuning* out);
+
+/* The context's current settings. */
+PBRCM_API int32_t pbrcm_tuning_get(pbrcm_context* ctx, pbrcm_tuning* out);
+/* Sets them (out-of-range values return PBRCM_ERR_ARG, nothing changed). */
+PBRCM_API int32_t pbrcm_tuning_set(pbrcm_context* ctx, const pbrcm_tuning* t);
+/* Applies a cache file written by pbrcm_autotune; PBRCM_ERR_NOT_FOUND if it
+ * is missing or was measured on another device shape or library version. */
+PBRCM_API int32_t pbrcm_tuning_load(pbrcm_context* ctx, const char* path);
 
 /* ---------------------------------------------------------------------- */
 /* Serving session: continuous batching of reorder requests.               */

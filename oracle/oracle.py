@@ -24,12 +24,12 @@ _u32p = ctypes.POINTER(ctypes.c_uint32)
 _lib = None
 
 
-def build(ref: bool = False) -> None:
-    """Builds the oracle library (and, if asked and the reference sources are
-    present, the reference driver) with oracle/Makefile."""
+def build(ref_dir: str | None = None) -> None:
+    """Builds the oracle library (and, given the reference's source tree, the
+    reference driver) with oracle/Makefile."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    if ref_dir:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_DIR={ref_dir}"], check=True)
 
 
 def lib():
@@ -237,6 +237,52 @@ def ref_time(rp, ci, threads: int, steps: int, timeout: float | None = None):
                             str(threads), str(steps)], capture_output=True, text=True, check=True,
                            timeout=timeout)
     return [json.loads(line[5:]) for line in r.stdout.splitlines() if line.startswith("JSON ")]
+
+
+def write_pack(path: str, mats) -> None:
+    """Writes CSRs [(row_ptr, col_idx), ...] as one pack file: u64 count, then
+    per matrix u64 n, u64 nnz, row_ptr (n+1 u32), col_idx (nnz u32)."""
+    with open(path, "wb") as f:
+        f.write(np.uint64(len(mats)).tobytes())
+        for rp, ci in mats:
+            rp, ci = _u32(rp), _u32(ci)
+            f.write(np.array([rp.shape[0] - 1, ci.shape[0]], dtype=np.uint64).tobytes())
+            f.write(rp.tobytes())
+            f.write(ci.tobytes())
+
+
+def ref_time_batch(mats, threads: int, reps: int = 1, timeout: float | None = None, want_perms: bool = False):
+    """The reference's findPeripheral + rcm_seq<true> over a stream of
+    matrices on `threads` host threads (oracle/_ref/ref_rcm timebatch), `reps`
+    times over the loaded graphs.  Returns (one info dict per rep with
+    wall_ms, start nodes, FNV-1a hashes of the CM orders) and, with
+    want_perms, a fourth item: the CM orders (one uint32 array per matrix)."""
+    with tempfile.TemporaryDirectory() as td:
+        pack = os.path.join(td, "pack")
+        write_pack(pack, mats)
+        out = os.path.join(td, "out")
+        r = subprocess.run([REF_BIN, "timebatch", pack, str(threads), out, str(reps)], capture_output=True,
+                           text=True, check=True, timeout=timeout)
+        info = [json.loads(line[5:]) for line in r.stdout.splitlines() if line.startswith("JSON ")]
+        raw = np.fromfile(out + ".hash", dtype=np.uint32).reshape(-1, 4)
+        allp = np.fromfile(out + ".perm", dtype=np.uint32) if want_perms else None
+    starts = raw[:, 0].copy()
+    hashes = raw[:, 2].astype(np.uint64) | (raw[:, 3].astype(np.uint64) << np.uint64(32))
+    if not want_perms:
+        return info, starts, hashes
+    ns = np.array([np.asarray(rp).shape[0] - 1 for rp, _ in mats], dtype=np.int64)
+    offs = np.concatenate([[0], np.cumsum(ns)])
+    perms = [allp[offs[i]:offs[i + 1]] for i in range(len(mats))]
+    return info, starts, hashes, perms
+
+
+def fnv1a_u32(a) -> int:
+    """FNV-1a over the u32 words of `a`, as ref_rcm timebatch hashes a
+    permutation."""
+    h = 1469598103934665603
+    for v in _u32(a).tolist():
+        h = ((h ^ v) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
 
 
 def permute_csr(rp, ci, perm, vals=None):

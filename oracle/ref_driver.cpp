@@ -24,22 +24,46 @@
 //       Times <steps> reorders: findPeripheral + RealCPU::rcm<true> with
 //       <threads> workers (1 = the serial rcm_seq path, else CPU_BATCH with
 //       batch size 512 as main.cpp:456-483 runs it).
+//   ref_rcm timebatch <pack> <threads> <outprefix> [reps]
+//       A stream of independent matrices (pack: u64 count, then per matrix
+//       u64 n, u64 nnz, row_ptr[n+1], col_idx[nnz]) reordered by <threads>
+//       host threads, each taking the next matrix: findPeripheral
+//       (simple_peripheral.cpp:92-141, thread-safe: its BFS state is
+//       thread_local) + one rcm_seq<true> (rcm_cpu.cpp:57-104, the serial
+//       stable path RealCPU::rcm<true> times).  The graphs are filled before
+//       the clock starts.  Prints the wall time of the pool; writes per
+//       matrix the start node and an FNV-1a hash of the permutation (CM
+//       order) to <outprefix>.hash (u32 start, u32 pad, u64 hash) and the
+//       permutations themselves, one after the other, to <outprefix>.perm.
+//       With [reps], the pool runs that many times over the loaded graphs,
+//       one JSON line each; the last repetition's permutations are kept.
 // `analyze` = findPeripheral (simple_peripheral.cpp:92) unless a start is
 // given, RealCPU::rcm<true>(.., 1, 1) (rcm_cpu.cpp:110), computeBandwidth /
 // checkBandwidth / maxValency / checkPermutation (main.cpp:94-226); it writes
 // the permutation to <outprefix>.perm and prints one line "JSON {...}".
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <iostream>
+#include <memory>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "Graph.h"
 #include "rcm_cpu.h"
 #include "simple_peripheral.h"
+
+// The reference's serial stable pass (rcm_cpu.cpp:57-104); rcm_cpu.cpp
+// instantiates it for float (through RealCPU::rcm<true>) as a weak symbol.
+namespace RealCPU {
+template <bool STABLE, typename T>
+void rcm_seq(Graph<T>& graph, std::vector<unsigned>& permutation, unsigned start_node);
+}
 
 // main.cpp (compiled with -Dmain=pbrcm_reference_cli_main)
 int computeBandwidth(const Graph<float>& graph, std::vector<uint32_t>& permutation);
@@ -128,6 +152,111 @@ double rcmTimed(Graph<float>& g, std::vector<unsigned>& perm, uint32_t start, un
     if (p != std::string::npos)
         ms = std::atof(s.c_str() + p + 10);
     return ms;
+}
+
+// One pass of the thread pool over every graph: findPeripheral + one
+// rcm_seq<true> per matrix, each thread taking the next index.  Returns the
+// wall time (ms); fills starts / hashes and the threads' summed busy time.
+double runPool(std::vector<std::unique_ptr<Graph<float>>>& graphs, unsigned threads, std::vector<uint32_t>& starts,
+               std::vector<uint64_t>& hashes, std::vector<std::vector<unsigned>>* keep, double& busy, int& failed)
+{
+    const uint64_t count = graphs.size();
+    std::vector<double> busy_ms(threads, 0.0);
+    std::atomic<uint64_t> next{0};
+    std::atomic<int> nfail{0};
+    // findPeripheral prints one line per call: std::cout goes nowhere while
+    // the pool runs (the buffer is swapped before any thread starts)
+    NullBuf nb;
+    auto* old = std::cout.rdbuf(&nb);
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (unsigned w = 0; w < threads; ++w) {
+        pool.emplace_back([&, w] {
+            NullBuf nb2;
+            std::ostream null_out(&nb2);
+            std::vector<unsigned> perm;
+            while (true) {
+                const uint64_t i = next.fetch_add(1);
+                if (i >= count)
+                    break;
+                auto a = std::chrono::steady_clock::now();
+                try {
+                    Graph<float>& g = *graphs[i];
+                    const uint32_t start = SimplePeripheral::findPeripheral(g, null_out, false);
+                    RealCPU::rcm_seq<true>(g, perm, start);
+                    uint64_t h = 1469598103934665603ull;
+                    for (unsigned v : perm)
+                        h = (h ^ v) * 1099511628211ull;
+                    starts[i] = start;
+                    hashes[i] = h;
+                    if (keep)
+                        std::swap((*keep)[i], perm);  // no copy; rcm_seq re-reserves
+                } catch (...) {
+                    nfail.fetch_add(1);
+                }
+                busy_ms[w] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+            }
+        });
+    }
+    for (auto& t : pool)
+        t.join();
+    const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    std::cout.rdbuf(old);
+    busy = 0.0;
+    for (double b : busy_ms)
+        busy += b;
+    failed = nfail.load();
+    return wall;
+}
+
+// timebatch: see the header.
+int timeBatch(const char* pack, unsigned threads, const std::string& outprefix, int reps)
+{
+    std::ifstream f(pack, std::ios::binary);
+    if (!f)
+        throw std::runtime_error(std::string("cannot open ") + pack);
+    uint64_t count = 0;
+    f.read(reinterpret_cast<char*>(&count), 8);
+    std::vector<std::unique_ptr<Graph<float>>> graphs;
+    uint64_t sum_nnz = 0;
+    for (uint64_t i = 0; i < count; ++i) {
+        uint64_t hdr[2];
+        f.read(reinterpret_cast<char*>(hdr), 16);
+        std::vector<uint32_t> rp(hdr[0] + 1), ci(hdr[1]);
+        f.read(reinterpret_cast<char*>(rp.data()), static_cast<std::streamsize>(rp.size() * 4));
+        f.read(reinterpret_cast<char*>(ci.data()), static_cast<std::streamsize>(ci.size() * 4));
+        if (!f)
+            throw std::runtime_error("truncated pack file");
+        graphs.emplace_back(new Graph<float>());
+        fillGraph(*graphs.back(), rp, ci);
+        sum_nnz += hdr[1];
+    }
+    threads = std::max(1u, threads);
+    std::vector<uint32_t> starts(count, 0);
+    std::vector<uint64_t> hashes(count, 0);
+    std::vector<std::vector<unsigned>> perms(count);
+    int failed_total = 0;
+    for (int rep = 0; rep < std::max(1, reps); ++rep) {
+        double busy = 0.0;
+        int failed = 0;
+        // the last repetition keeps its permutations
+        const bool last = rep + 1 == std::max(1, reps);
+        const double wall = runPool(graphs, threads, starts, hashes, last ? &perms : nullptr, busy, failed);
+        failed_total += failed;
+        std::printf("JSON {\"rep\": %d, \"count\": %llu, \"sum_nnz\": %llu, \"threads\": %u, \"wall_ms\": %.4f, "
+                    "\"busy_ms\": %.4f, \"failed\": %d}\n",
+                    rep, (unsigned long long)count, (unsigned long long)sum_nnz, threads, wall, busy, failed);
+        std::fflush(stdout);
+    }
+    std::ofstream o(outprefix + ".hash", std::ios::binary);
+    std::ofstream op(outprefix + ".perm", std::ios::binary);
+    for (uint64_t i = 0; i < count; ++i) {
+        const uint32_t w2[2] = {starts[i], 0u};
+        o.write(reinterpret_cast<const char*>(w2), 8);
+        o.write(reinterpret_cast<const char*>(&hashes[i]), 8);
+        op.write(reinterpret_cast<const char*>(perms[i].data()), static_cast<std::streamsize>(perms[i].size() * 4));
+    }
+    return failed_total ? 4 : 0;
 }
 
 int analyze(Graph<float>& g, const std::string& outprefix, long forced_start)
@@ -236,11 +365,14 @@ int main(int argc, char** argv)
             }
             return 0;
         }
+        if (argc >= 5 && std::strcmp(argv[1], "timebatch") == 0)
+            return timeBatch(argv[2], static_cast<unsigned>(std::atoi(argv[3])), argv[4],
+                             argc >= 6 ? std::atoi(argv[5]) : 1);
     } catch (std::exception& e) {
         std::printf("JSON {\"error\": \"%s\"}\n", e.what());
         return 3;
     }
     std::fprintf(stderr, "usage: ref_rcm load <mtx> <outprefix> [start] | csr <rp> <ci> <outprefix> [start] | "
-                         "time <rp> <ci> <threads> <steps>\n");
+                         "time <rp> <ci> <threads> <steps> | timebatch <pack> <threads> <outprefix> [reps]\n");
     return 1;
 }

@@ -12,7 +12,7 @@ from .rcm import (  # noqa: F401
     load_hicsr, load_mtx,
     max_valency, store_hicsr,
     permute, permute_device, prepare_csr, reorder, reorder_batch, reorder_batch_device, reorder_device,
-    reorder_device_noalloc, store_mtx,
+    reorder_device_noalloc, store_mtx, autotune, tuning_get, tuning_set, tuning_load,
 )
 
 __version__ = "0.1.0"

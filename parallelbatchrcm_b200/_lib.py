@@ -67,6 +67,19 @@ class SessionStats(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ("batch_pool", ctypes.c_uint32), ("cluster_size", ctypes.c_uint32), ("cluster_max", ctypes.c_uint32),
+        ("cluster_nnz", ctypes.c_uint32), ("session_cutoff_n", ctypes.c_uint32), ("session_pool", ctypes.c_uint32),
+        ("sms", ctypes.c_uint32),
+        ("trials", ctypes.c_uint32), ("source", ctypes.c_uint32), ("default_ms", ctypes.c_float),
+        ("best_ms", ctypes.c_float), ("session_default_ms", ctypes.c_float), ("session_best_ms", ctypes.c_float),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 # every symbol include/pbrcm.h declares, with (restype, argtypes)
 _vp = ctypes.c_void_p
 _u32 = ctypes.c_uint32
@@ -112,6 +125,11 @@ SIGNATURES = {
                                 ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)),
                                 ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)), ctypes.POINTER(_vp), _pu32]),
     "pbrcm_store_hicsr": (_i32, [ctypes.c_char_p, _u32, _u64, _vp, _vp, _vp, _u32]),
+    "pbrcm_autotune": (_i32, [_vp, ctypes.POINTER(Matrix), _u32, ctypes.POINTER(Options), ctypes.c_char_p,
+                              ctypes.POINTER(Tuning)]),
+    "pbrcm_tuning_get": (_i32, [_vp, ctypes.POINTER(Tuning)]),
+    "pbrcm_tuning_set": (_i32, [_vp, ctypes.POINTER(Tuning)]),
+    "pbrcm_tuning_load": (_i32, [_vp, ctypes.c_char_p]),
 }
 
 _lib = None

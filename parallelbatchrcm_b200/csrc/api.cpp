@@ -114,6 +114,15 @@ int32_t Context::init(int dev)
         return PBRCM_ERR_CUDA;
     if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess)
         return PBRCM_ERR_CUDA;
+    // host-buffer batches copy their inputs on a second stream while the
+    // batch kernel already runs
+    if (cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess)
+        return PBRCM_ERR_CUDA;
+    if (cudaMallocHost(&h_one, sizeof(uint32_t)) != cudaSuccess)
+        return PBRCM_ERR_OOM;
+    *h_one = 1u;
     if (cudaMalloc(&d_res, sizeof(DevResult)) != cudaSuccess || cudaMalloc(&d_gs, kTeamParts * sizeof(GridSync)) != cudaSuccess)
         return PBRCM_ERR_OOM;
     if (cudaMallocHost(&h_res, sizeof(DevResult)) != cudaSuccess ||
@@ -146,20 +155,40 @@ int32_t Context::init(int dev)
     wide_fused = env_int("PBRCM_WIDE_FUSED", 1) != 0;
     wide_batch_pass = env_int("PBRCM_WIDE_BATCH_PASS", 1) != 0;
     wide_ctas = wide_ctas_per_sm() * sms;
-    batch_variant = env_int("PBRCM_BATCH_VARIANT", 2);
-    if (batch_variant < 0 || batch_variant >= kNumVariants)
-        batch_variant = 2;
+    // batch / serving shape: built-in defaults (measured on the 4,096-matrix
+    // mixed batch: 212 / 178 / 220 / 382 ms for 1 x 512, 2 x 256, 4 x 128,
+    // 8 x 64 threads per group), or a tuning file written by pbrcm_autotune
+    // for this device shape and library version (PBRCM_TUNING); a PBRCM_*
+    // knob below still overrides a single setting
+    pbrcm_tuning tn;
+    std::memset(&tn, 0, sizeof(tn));
+    tn.batch_pool = 1;
+    tn.cluster_size = 2;
+    tn.cluster_max = 16;
+    tn.cluster_nnz = 1u << 18;
+    tn.session_cutoff_n = 1u << 18;
+    tn.session_pool = 0;
+    if (const char* tp = std::getenv("PBRCM_TUNING")) {
+        if (load_tuning_file(tp, sms, &tn))
+            tuned = 1;
+    }
+    batch_pool = env_int("PBRCM_BATCH_POOL", (int)tn.batch_pool);
+    if (batch_pool < 0 || batch_pool > 3)
+        batch_pool = 1;
+    session_cutoff_n = (uint32_t)std::max(1, env_int("PBRCM_SESSION_CUTOFF_N", (int)tn.session_cutoff_n));
+    session_pool = env_int("PBRCM_SESSION_POOL", (int)tn.session_pool) == 4 ? 4 : 0;
+    solo = env_int("PBRCM_SOLO", 0) != 0;
     if (cudaMalloc(&d_agg, kTeamParts * team_part_bytes(maxc)) != cudaSuccess)
         return PBRCM_ERR_OOM;
     // cluster teams of the batch path (PBRCM_BATCH_CLUSTER* override)
     // measured on the mixed 1,024-matrix batch: pairs for the 16 biggest
     // matrices cut its makespan by ~16 %; larger clusters or more of them
     // cost more CTA-time than the tail they remove
-    cluster_size = env_int("PBRCM_BATCH_CLUSTER", 2);
-    cluster_nnz = (uint64_t)std::max(1, env_int("PBRCM_BATCH_CLUSTER_NNZ", 1 << 18));
-    cluster_max = env_int("PBRCM_BATCH_CLUSTERS", 16);
-    cluster_solo_parents = (uint32_t)env_int("PBRCM_CLUSTER_SOLO_PARENTS", kVariants[batch_variant].block);
-    cluster_solo_edges = (uint32_t)env_int("PBRCM_CLUSTER_SOLO_EDGES", kVariants[batch_variant].emax);
+    cluster_size = env_int("PBRCM_BATCH_CLUSTER", (int)tn.cluster_size);
+    cluster_nnz = (uint64_t)std::max(1, env_int("PBRCM_BATCH_CLUSTER_NNZ", (int)tn.cluster_nnz));
+    cluster_max = env_int("PBRCM_BATCH_CLUSTERS", (int)tn.cluster_max);
+    cluster_solo_parents = (uint32_t)env_int("PBRCM_CLUSTER_SOLO_PARENTS", kPools[batch_pool].block);
+    cluster_solo_edges = (uint32_t)env_int("PBRCM_CLUSTER_SOLO_EDGES", kPools[batch_pool].emax);
     return PBRCM_OK;
 }
 
@@ -174,6 +203,18 @@ Context::~Context()
                     (void*)d_arena})
         if (p)
             cudaFree(p);
+    if (d_ready)
+        cudaFree(d_ready);
+    if (h_one)
+        cudaFreeHost(h_one);
+    if (ev_fork)
+        cudaEventDestroy(ev_fork);
+    if (ev_join)
+        cudaEventDestroy(ev_join);
+    if (copy_stream) {
+        cudaStreamSynchronize(copy_stream);
+        cudaStreamDestroy(copy_stream);
+    }
     if (h_res)
         cudaFreeHost(h_res);
     if (h_aux)

@@ -3,13 +3,16 @@
 //
 // Layout: one device arena per call holds, per matrix, its CSR (host-input
 // form only), its node table node[n], rec[n] and perm[n] (host-input form
-// only), each 16-byte aligned.  Jobs are ordered by nnz, biggest first; a
-// job above the team threshold gets a team of K CTAs (K grows with its nnz)
-// with its own zeroed barrier words, the others one CTA.  The work list
-// holds K consecutive slots per job; k_reorder_batch (a cooperative launch,
-// so that every CTA is resident and a team always fills up) hands the slots
-// out with an atomic counter.  Every CTA of a job runs the whole reorder of
-// that matrix (start search, CM pass, reverse, bandwidth).
+// only), each 16-byte aligned.  Jobs are ordered by nnz, biggest first.  The
+// biggest (nnz >= cluster_nnz, at most cluster_max of them) are reordered by
+// thread-block-cluster teams of whole CTAs; every other job takes one slot
+// of the work list, which the CTAs' thread groups (several per CTA, the
+// context's pool shape) hand out with an atomic counter, so that several
+// matrices are in flight on every SM.  (With PBRCM_BATCH_TEAM_MAX > 1 a big
+// job instead gets a team of K groups with its own zeroed barrier words and
+// K consecutive slots, in a cooperative launch.)  Every group of a job runs
+// the whole reorder of that matrix (start search, CM pass, reverse,
+// bandwidth).
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -31,7 +34,7 @@ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 inline size_t align128(size_t x) { return (x + 127) & ~(size_t)127; }
 
 struct Slot {
-    size_t rp, ci, node, rec, perm;  // arena offsets (rp/ci/perm unused for device input)
+    size_t rp, ci, node, rec, perm, e2;  // arena offsets (rp/ci/perm unused for device input; e2 0: none)
 };
 
 int env_int(const char* name, int dflt)
@@ -65,15 +68,17 @@ uint32_t team_size(uint64_t nnz, uint64_t min_nnz, uint64_t nnz_per_cta, uint32_
     return (uint32_t)std::max<uint64_t>(2, std::min<uint64_t>(k, max_team));
 }
 
+}  // namespace
+
 // Shared driver; `host` selects whether mats[] point to host or device memory.
-int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pbrcm_options* opts,
-                  pbrcm_result* results, cudaStream_t st, bool host)
+int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pbrcm_options* opts,
+                         pbrcm_result* results, cudaStream_t st, bool host)
 {
     auto t0 = std::chrono::steady_clock::now();
     Options opt = make_options(opts, kModeFull);
-    const int v = C.batch_variant;
-    opt.solo_parents = 2 * kVariants[v].block;
-    opt.solo_edges = 2 * kVariants[v].emax;
+    const int v = C.batch_pool;
+    opt.solo_parents = 2 * kPools[v].group;
+    opt.solo_edges = 2 * kPools[v].gemax;
     opt.barrier = 0;
     for (uint32_t j = 0; j < count; ++j) {
         const pbrcm_matrix& m = mats[j];
@@ -120,16 +125,21 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
         if (team[q] > 1)
             teamws = align128(teamws + sizeof(GridSync)) + align128(team_words_bytes((int)team[q]));
     }
-    // arena layout
+    // arena layout, in job order (biggest first); every CSR on a 128-byte
+    // boundary so that no cache line holds two matrices' data (a host-buffer
+    // batch's CSRs arrive while other matrices are already being read)
     std::vector<Slot> slot(count);
     size_t off = 0;
-    for (uint32_t j = 0; j < count; ++j) {
+    size_t in_bytes = 0;
+    for (uint32_t q = 0; q < count; ++q) {
+        const uint32_t j = order[q];
         const pbrcm_matrix& m = mats[j];
         if (host) {
             slot[j].rp = off;
-            off = align16(off + 4 * ((size_t)m.n + 1));
+            off = align128(off + 4 * ((size_t)m.n + 1));
             slot[j].ci = off;
-            off = align16(off + 4 * (size_t)m.nnz);
+            off = align128(off + 4 * (size_t)m.nnz);
+            in_bytes += 4 * ((size_t)m.n + 1) + 4 * (size_t)m.nnz;
         }
         slot[j].node = off;
         off = align16(off + 16 * (size_t)m.n);
@@ -139,24 +149,42 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
             slot[j].perm = off;
             off = align16(off + 4 * (size_t)m.n);
         }
+        // the one-group engine's edge records (16 bytes per entry) for a
+        // matrix a single group will take and whose visited set fits shared
+        // memory; it uses the node table's room for its inverse permutation
+        slot[j].e2 = 0;
+        if (C.solo && q >= nbig && team[q] == 1 && m.n <= kSoloMaxN && m.nnz > 0) {
+            off = align16(off);
+            slot[j].e2 = off;
+            off += 16 * (size_t)m.nnz;
+        }
+        off = align128(off);
     }
     const size_t team_off = align128(off);
     off = team_off + teamws;
-    if (!grow_dev(C.d_arena, C.cap_arena, off) || !grow_dev(C.d_jobs, C.cap_jobs, count) ||
-        !grow_dev(C.d_bres, C.cap_bres, count) || !grow_dev(C.d_slots, C.cap_slots, nslots) ||
-        !grow_dev(C.d_counter, C.cap_counter, 8))
-        return PBRCM_ERR_OOM;
-    unsigned char* A = C.d_arena;
+    // host buffers: the CSRs go in waves of about in_bytes / kWaves in job
+    // order, each wave followed by its ready word, while the kernel runs
+    constexpr size_t kWaves = 48;
+    const size_t wave_bytes = std::max<size_t>(in_bytes / kWaves, (size_t)4 << 20);
+    std::vector<uint32_t> wave(count, 0);
+    uint32_t nwaves = 0;
     if (host) {
-        for (uint32_t j = 0; j < count; ++j) {
-            const pbrcm_matrix& m = mats[j];
-            if (cudaMemcpyAsync(A + slot[j].rp, m.row_ptr, 4 * ((size_t)m.n + 1), cudaMemcpyHostToDevice, st) !=
-                    cudaSuccess ||
-                (m.nnz && cudaMemcpyAsync(A + slot[j].ci, m.col_idx, 4 * (size_t)m.nnz, cudaMemcpyHostToDevice,
-                                          st) != cudaSuccess))
-                return PBRCM_ERR_CUDA;
+        size_t cum = 0;
+        for (uint32_t q = 0; q < count; ++q) {
+            const pbrcm_matrix& m = mats[order[q]];
+            wave[q] = nwaves;
+            cum += 4 * ((size_t)m.n + 1) + 4 * (size_t)m.nnz;
+            if (cum >= wave_bytes || q + 1 == count) {
+                ++nwaves;
+                cum = 0;
+            }
         }
     }
+    if (!grow_dev(C.d_arena, C.cap_arena, off) || !grow_dev(C.d_jobs, C.cap_jobs, count) ||
+        !grow_dev(C.d_bres, C.cap_bres, count) || !grow_dev(C.d_slots, C.cap_slots, nslots) ||
+        !grow_dev(C.d_counter, C.cap_counter, 8) || (nwaves && !grow_dev(C.d_ready, C.cap_ready, nwaves)))
+        return PBRCM_ERR_OOM;
+    unsigned char* A = C.d_arena;
     std::vector<BatchJob> jobs(count);
     std::vector<BatchSlot> slots;
     slots.reserve(nslots);
@@ -176,6 +204,9 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
         J.M.hub = nullptr;
         J.M.res = C.d_bres + q;
         J.team = q < nbig ? 1 : team[q];
+        J.ready = host ? C.d_ready + wave[q] : nullptr;
+        J.e2 = slot[j].e2 ? reinterpret_cast<uint4*>(A + slot[j].e2) : nullptr;
+        J.inv = reinterpret_cast<uint32_t*>(A + slot[j].node);
         if (team[q] > 1) {
             J.gs = reinterpret_cast<GridSync*>(A + tw);
             tw = align128(tw + sizeof(GridSync));
@@ -190,10 +221,16 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
         cudaMemcpyAsync(C.d_slots, slots.data(), sizeof(BatchSlot) * nslots, cudaMemcpyHostToDevice, st) !=
             cudaSuccess ||
         (teamws && cudaMemsetAsync(A + team_off, 0, teamws, st) != cudaSuccess) ||
+        (nwaves && cudaMemsetAsync(C.d_ready, 0, sizeof(uint32_t) * nwaves, st) != cudaSuccess) ||
         cudaMemsetAsync(C.d_bres, 0, sizeof(DevResult) * count, st) != cudaSuccess ||
         cudaMemsetAsync(C.d_counter, 0, 2 * sizeof(uint32_t), st) != cudaSuccess)
         return PBRCM_ERR_CUDA;
-    if (launch_validate_batch(C.d_jobs, count, C.sms, st) != cudaSuccess)
+    // the wait for a wave is bounded; the bound grows with the bytes to copy
+    // (at least 1 GB/s)
+    opt.data_wait_ns = opt.wait_ns + (unsigned long long)in_bytes;
+    // the copy stream starts once the ready words are zeroed (fork)
+    if (host && (cudaEventRecord(C.ev_fork, st) != cudaSuccess ||
+                 cudaStreamWaitEvent(C.copy_stream, C.ev_fork, 0) != cudaSuccess))
         return PBRCM_ERR_CUDA;
     cudaEventRecord(C.ev0, st);
     if (nbig) {
@@ -204,9 +241,34 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
                            ncl, st) != cudaSuccess)
             return PBRCM_ERR_CUDA;
     } else {
-        const int ctas = std::max(1, std::min<int>(maxc, (int)nslots));
+        const uint32_t per_cta = (uint32_t)(kPools[v].block / kPools[v].group);
+        const int ctas = std::max(1, std::min<int>(maxc, (int)((nslots + per_cta - 1) / per_cta)));
         if (launch_batch(v, C.d_jobs, C.d_slots, (uint32_t)nslots, C.d_counter, opt, ctas, nslots > count, st) !=
             cudaSuccess)
+            return PBRCM_ERR_CUDA;
+    }
+    if (host) {
+        // the inputs, wave by wave, each wave's ready word after its CSRs
+        // (copies on one stream complete in order); the kernel above waits
+        // for each matrix's wave
+        cudaStream_t cs = C.copy_stream;
+        uint32_t q = 0;
+        bool ok = true;
+        for (uint32_t w = 0; w < nwaves && ok; ++w) {
+            for (; q < count && wave[q] == w && ok; ++q) {
+                const pbrcm_matrix& m = mats[order[q]];
+                const Slot& sl = slot[order[q]];
+                ok = cudaMemcpyAsync(A + sl.rp, m.row_ptr, 4 * ((size_t)m.n + 1), cudaMemcpyHostToDevice, cs) ==
+                         cudaSuccess &&
+                     (!m.nnz || cudaMemcpyAsync(A + sl.ci, m.col_idx, 4 * (size_t)m.nnz, cudaMemcpyHostToDevice,
+                                                cs) == cudaSuccess);
+            }
+            ok = ok && cudaMemcpyAsync(C.d_ready + w, C.h_one, sizeof(uint32_t), cudaMemcpyHostToDevice, cs) ==
+                           cudaSuccess;
+        }
+        // join: nothing after the kernel runs before the copies are done
+        if (!ok || cudaEventRecord(C.ev_join, cs) != cudaSuccess ||
+            cudaStreamWaitEvent(st, C.ev_join, 0) != cudaSuccess)
             return PBRCM_ERR_CUDA;
     }
     cudaEventRecord(C.ev1, st);
@@ -237,6 +299,12 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
             cudaStreamSynchronize(st) != cudaSuccess)
             return PBRCM_ERR_CUDA;
     }
+    // per-matrix latency inside the batch: from the first matrix taken to
+    // this one's result (device %globaltimer)
+    unsigned long long tmin = ~0ull;
+    for (uint32_t q = 0; q < count; ++q)
+        if (res[q].t_begin)
+            tmin = std::min(tmin, res[q].t_begin);
     int32_t worst = PBRCM_OK;
     for (uint32_t q = 0; q < count; ++q) {
         const uint32_t j = order[q];
@@ -247,7 +315,8 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
         }
         if (results) {
             fill_result(res[q], opt, &results[j]);
-            results[j].device_ms = dms;
+            results[j].device_ms = res[q].t_end >= tmin && tmin != ~0ull ? (float)((res[q].t_end - tmin) * 1e-6)
+                                                                          : dms;
         }
         if (res[q].status != kOk && worst == PBRCM_OK)
             worst = map_status(res[q].status);
@@ -261,8 +330,6 @@ int32_t run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pb
     }
     return worst;
 }
-
-}  // namespace
 
 extern "C" {
 

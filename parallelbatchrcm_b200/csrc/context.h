@@ -19,7 +19,8 @@ struct Context {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int team_variant = 1;   // kernel shape of the one-matrix team
     int team_ctas = 0;      // CTAs of the one-matrix team
-    int batch_variant = 2;  // kernel shape of the batch kernel
+    int batch_pool = 1;     // shape of the batch kernels (kPools: CTA and group sizes)
+    bool solo = true;       // batch: one-group jobs run the solo engine where it applies (PBRCM_SOLO=0: never)
     uint32_t solo_edges = 0;    // levels at most this big run on one CTA
     uint32_t solo_parents = 0;
     uint32_t barrier = 0;       // team barrier implementation
@@ -38,6 +39,12 @@ struct Context {
     uint64_t cluster_nnz = 1u << 18;  // matrices with at least this many entries
     int cluster_max = 16;             // cap on the matrices given a cluster (0: one per co-resident cluster)
     uint32_t cluster_solo_parents = 0, cluster_solo_edges = 0;  // solo level bounds inside a cluster
+    // serving: a request of more nodes runs on a cooperative team
+    uint32_t session_cutoff_n = 1u << 18;
+    int session_pool = 0;  // serving: kPools shape of the one-CTA requests
+    // where the batch / serving shape came from: 0 built-in defaults, 1 a
+    // tuning file, 2 pbrcm_autotune or pbrcm_tuning_set
+    uint32_t tuned = 0;
 
     // single-matrix buffers (grow only)
     uint32_t* d_rp = nullptr;
@@ -79,6 +86,13 @@ struct Context {
     size_t cap_bres = 0;
     unsigned char* d_arena = nullptr;
     size_t cap_arena = 0;
+    // host-buffer batches: inputs copied in waves on copy_stream, each wave
+    // followed by a copy of *h_one into its ready word d_ready[w]
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    uint32_t* d_ready = nullptr;
+    size_t cap_ready = 0;
+    uint32_t* h_one = nullptr;
 
     int32_t init(int dev);
     ~Context();
@@ -98,6 +112,15 @@ struct Context {
     // false on a CUDA error; M.res holds the outcome (kNeedTeam: use the team)
     bool run_wide(const MatrixView& M, const Options& opt, cudaStream_t st);
 };
+
+// The many-matrix driver (batch.cpp); `host` selects whether mats[] point
+// to host or device memory.
+int32_t run_batch(Context& C, const struct pbrcm_matrix* mats, uint32_t count, const struct pbrcm_options* opts,
+                  struct pbrcm_result* results, cudaStream_t st, bool host);
+// The shape settings a tuning holds (tune.cpp): read by Context::init from
+// the file named by PBRCM_TUNING when its key matches this device and
+// library, before the environment knobs (which still override).
+bool load_tuning_file(const char* path, int sms, struct pbrcm_tuning* out);
 
 int32_t map_status(uint32_t s);
 Options make_options(const struct pbrcm_options* o, uint32_t mode);

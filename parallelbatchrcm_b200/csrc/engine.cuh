@@ -125,6 +125,52 @@ __device__ __forceinline__ uint32_t read_status(const DevResult* r)
 #define PB_CHECK(res, cond, where) true
 #endif
 
+// ---------------------------------------------------------------------------
+// Thread groups.  One engine instance runs on a group of B consecutive
+// threads of a CTA: the whole CTA, or one of blockDim.x / B equal slices, so
+// that one CTA can reorder several matrices at once.  Group g synchronises on
+// named barrier 1 + g (barrier 0 stays the CTA-wide __syncthreads); every
+// engine barrier is reached by all B threads of the group, never by a
+// diverged subset.
+// ---------------------------------------------------------------------------
+template <int B>
+__device__ __forceinline__ uint32_t gtid()
+{
+    static_assert(B >= 32 && B <= 1024 && (B & (B - 1)) == 0, "groups are a power-of-two number of warps");
+    return threadIdx.x & (B - 1);
+}
+
+template <int B>
+__device__ __forceinline__ uint32_t gbar_id()
+{
+    return 1u + threadIdx.x / B;
+}
+
+template <int B>
+__device__ __forceinline__ void gsync()
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(gbar_id<B>()), "n"(B) : "memory");
+}
+
+// Group barrier that also counts the threads whose predicate holds.
+template <int B>
+__device__ __forceinline__ int gsync_count(bool pred)
+{
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.popc.u32 %0, %2, %3, p;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(gbar_id<B>()), "n"(B)
+        : "memory");
+    return r;
+}
+
+// Barrier of a group given at run time (id, threads).
+__device__ __forceinline__ void gsync_n(uint32_t id, uint32_t nthr)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthr) : "memory");
+}
+
 // Block-wide exclusive scan of one value per thread (T = uint32_t or
 // unsigned long long).  `tmp` holds B/32 + 1 entries.  Ends with a barrier,
 // so `tmp` can be reused right away.
@@ -132,7 +178,7 @@ template <int B, typename T>
 __device__ __forceinline__ T block_exclusive_scan(T v, T& total, T* tmp)
 {
     constexpr int W = B / 32;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, w = gtid<B>() >> 5;
     T x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -142,7 +188,7 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T& total, T* tmp)
     }
     if (lane == 31)
         tmp[w] = x;
-    __syncthreads();
+    gsync<B>();
     if (w == 0) {
         T s = lane < W ? tmp[lane] : T(0);
 #pragma unroll
@@ -154,10 +200,10 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T& total, T* tmp)
         if (lane < W)
             tmp[lane] = s;
     }
-    __syncthreads();
+    gsync<B>();
     T r = (w ? tmp[w - 1] : T(0)) + x - v;
     total = tmp[W - 1];
-    __syncthreads();
+    gsync<B>();
     return r;
 }
 
@@ -168,7 +214,7 @@ template <int B>
 __device__ __forceinline__ uint32_t block_scan1(uint32_t v, uint32_t& total, uint32_t* buf)
 {
     constexpr int W = B / 32;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, w = gtid<B>() >> 5;
     uint32_t x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -178,7 +224,7 @@ __device__ __forceinline__ uint32_t block_scan1(uint32_t v, uint32_t& total, uin
     }
     if (lane == 31)
         buf[w] = x;
-    __syncthreads();
+    gsync<B>();
     uint32_t before = 0, all = 0;
 #pragma unroll
     for (int i = 0; i < W; ++i) {
@@ -194,7 +240,7 @@ template <int B, typename T>
 __device__ __forceinline__ T block_reduce_max(T v, T* tmp)
 {
     constexpr int W = B / 32;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, w = gtid<B>() >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         T y = __shfl_xor_sync(kFull, v, o);
@@ -202,11 +248,11 @@ __device__ __forceinline__ T block_reduce_max(T v, T* tmp)
     }
     if (lane == 0)
         tmp[w] = v;
-    __syncthreads();
+    gsync<B>();
     T r = tmp[0];
     for (int i = 1; i < W; ++i)
         r = r > tmp[i] ? r : tmp[i];
-    __syncthreads();
+    gsync<B>();
     return r;
 }
 
@@ -214,17 +260,17 @@ template <int B, typename T>
 __device__ __forceinline__ T block_reduce_sum(T v, T* tmp)
 {
     constexpr int W = B / 32;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, w = gtid<B>() >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
         v += __shfl_xor_sync(kFull, v, o);
     if (lane == 0)
         tmp[w] = v;
-    __syncthreads();
+    gsync<B>();
     T r = 0;
     for (int i = 0; i < W; ++i)
         r += tmp[i];
-    __syncthreads();
+    gsync<B>();
     return r;
 }
 
@@ -234,7 +280,7 @@ __device__ __forceinline__ void block_reduce_sum2(unsigned long long& a, unsigne
                                                   unsigned long long* tmp)
 {
     constexpr int W = B / 32;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, w = gtid<B>() >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         a += __shfl_xor_sync(kFull, a, o);
@@ -244,7 +290,7 @@ __device__ __forceinline__ void block_reduce_sum2(unsigned long long& a, unsigne
         tmp[w] = a;
         tmp[W + w] = b;
     }
-    __syncthreads();
+    gsync<B>();
     unsigned long long ra = 0, rb = 0;
     for (int i = 0; i < W; ++i) {
         ra += tmp[i];
@@ -252,10 +298,12 @@ __device__ __forceinline__ void block_reduce_sum2(unsigned long long& a, unsigne
     }
     a = ra;
     b = rb;
-    __syncthreads();
+    gsync<B>();
 }
 
 // Level state of one pass, the same in every CTA of a team.
+constexpr int kTeamShared = 12;  // group-shared ints a team needs (Team::sh)
+
 struct LevelState {
     uint32_t a, b;     // frontier positions [a, b)
     uint32_t Ka, Kb;   // edge ids of the frontier [Ka, Kb)
@@ -279,16 +327,23 @@ struct Team {
     uint32_t epoch;      // gate epochs seen
     unsigned long long wait_ns;
     DevResult* res;
+    // the thread group running this CTA's part (see gtid): its thread 0 is
+    // tid == 0, its barrier is (bar, nthr); sh holds kTeamShared ints of
+    // group-shared scratch, one slot per function so that one function's
+    // result can still be read while the next one writes its own
+    uint32_t tid, bar, nthr;
+    int* sh;
 
-    // Block-uniform "keep going?" after a block barrier.
+    __device__ __forceinline__ void gbar() const { gsync_n(bar, nthr); }
+
+    // Group-uniform "keep going?" after a group barrier.
     __device__ bool block_ok()
     {
-        __shared__ int s_ok;
-        __syncthreads();
-        if (threadIdx.x == 0)
-            s_ok = read_status(res) == 0;
-        __syncthreads();
-        return s_ok != 0;
+        gbar();
+        if (tid == 0)
+            sh[0] = read_status(res) == 0;
+        gbar();
+        return sh[0] != 0;
     }
 
     // Team barrier, two implementations (Options::barrier):
@@ -301,15 +356,15 @@ struct Team {
     // ran out).
     __device__ bool sync(uint32_t where)
     {
-        __shared__ int s_ok;
+        int& s_ok = sh[1];
         if (gs == nullptr)
             return block_ok();
         target += 1;
-        if (threadIdx.x == 0)
+        if (tid == 0)
             s_ok = 1;
-        __syncthreads();
+        gbar();
         if (mode == 0) {
-            if (threadIdx.x == 0) {
+            if (tid == 0) {
                 red_release_add(&gs->count, 1u);
                 const uint32_t goal = target * expected;
                 unsigned long long t0 = 0;
@@ -324,9 +379,9 @@ struct Team {
                 }
             }
         } else {
-            if (threadIdx.x == 0)
+            if (tid == 0)
                 st_release(flags + rank, target);
-            for (uint32_t i = threadIdx.x; i < expected; i += blockDim.x) {
+            for (uint32_t i = tid; i < expected; i += nthr) {
                 unsigned long long t0 = 0;
                 uint32_t spins = 0;
                 while ((int)(*reinterpret_cast<volatile unsigned int*>(flags + i) - target) < 0) {
@@ -340,9 +395,9 @@ struct Team {
                 __threadfence();
             }
         }
-        __syncthreads();
+        gbar();
         const int ok = s_ok && read_status(res) == 0;
-        __syncthreads();
+        gbar();
         return ok != 0;
     }
 
@@ -365,7 +420,7 @@ struct Team {
     // Heartbeat of CTA 0's solo run (keeps the gate waiters' bound fresh).
     __device__ __forceinline__ void beat()
     {
-        if (gs != nullptr && threadIdx.x == 0)
+        if (gs != nullptr && tid == 0)
             atomicAdd(&gs->heartbeat, 1u);
     }
 
@@ -373,10 +428,10 @@ struct Team {
     // polls; the wait only runs out if CTA 0's heartbeat stops for wait_ns.
     __device__ bool gate_wait(LevelState& st)
     {
-        __shared__ int s_ok;
-        __shared__ uint32_t s_st[6];
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        int& s_ok = sh[2];
+        int* s_st = sh + 3;  // 6 slots
+        gbar();
+        if (tid == 0) {
             int ok = 1;
             const uint32_t want = epoch + 1;
             unsigned long long t0 = globaltimer();
@@ -404,10 +459,10 @@ struct Team {
             }
             if (ok)
                 for (int i = 0; i < 6; ++i)
-                    s_st[i] = __ldcg(&gs->st[i]);
+                    s_st[i] = (int)__ldcg(&gs->st[i]);
             s_ok = ok && read_status(res) == 0;
         }
-        __syncthreads();
+        gbar();
         epoch += 1;
         if (s_ok) {
             st.a = s_st[0];
@@ -424,8 +479,8 @@ struct Team {
     // team goes on (the waiters read the error status themselves).
     __device__ bool gate_open(const LevelState& st, bool ok)
     {
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        gbar();
+        if (tid == 0) {
             gs->st[0] = st.a;
             gs->st[1] = st.b;
             gs->st[2] = st.Ka;
@@ -435,7 +490,7 @@ struct Team {
             __threadfence();
             st_release(&gs->epoch, epoch + 1);
         }
-        __syncthreads();
+        gbar();
         epoch += 1;
         return ok;
     }
@@ -444,7 +499,7 @@ struct Team {
     // with the level's step number.
     __device__ __forceinline__ void ag_publish(uint32_t cnt, uint32_t esum, uint32_t step, unsigned long long* agg)
     {
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             st_relaxed64(agg + 2 * rank, ((unsigned long long)step << 32) | cnt);
             st_relaxed64(agg + 2 * rank + 1, ((unsigned long long)step << 32) | esum);
         }
@@ -456,13 +511,13 @@ struct Team {
     __device__ bool ag_collect(uint32_t step, const unsigned long long* agg, unsigned long long& pre,
                                unsigned long long& all, unsigned long long* red)
     {
-        __shared__ int s_ok;
-        const uint32_t t = threadIdx.x;
+        int& s_ok = sh[9];
+        const uint32_t t = tid;
         pre = 0;
         all = 0;
         if (t == 0)
             s_ok = 1;
-        __syncthreads();
+        gbar();
         for (uint32_t i = t; i < size; i += B) {
             unsigned long long vc, ve;
             unsigned long long t0 = 0;
@@ -504,6 +559,7 @@ struct ClusterShared {
     uint32_t st[6];               // CTA 0: level state handed over at the gate
     uint32_t job;                 // CTA 0: the job the cluster works on
     uint32_t all_ok;              // this CTA's AND of the peers' flags
+    uint32_t job_ok;              // this CTA's verdict on the job (CSR arrived and valid, no hub)
 };
 
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
@@ -516,6 +572,12 @@ struct ClusterTeam {
     uint32_t rank;      // this CTA's rank in the cluster
     uint32_t phase;     // cluster barriers passed (slot parity)
     DevResult* res;
+    // the CTA's thread group (a cluster team always spans whole CTAs) and
+    // its group-shared scratch, as in Team
+    uint32_t tid, bar, nthr;
+    int* sh;
+
+    __device__ __forceinline__ void gbar() const { gsync_n(bar, nthr); }
 
     __device__ __forceinline__ ClusterShared* peer(uint32_t r) const
     {
@@ -524,12 +586,11 @@ struct ClusterTeam {
 
     __device__ bool block_ok()
     {
-        __shared__ int s_ok;
-        __syncthreads();
-        if (threadIdx.x == 0)
-            s_ok = read_status(res) == 0;
-        __syncthreads();
-        return s_ok != 0;
+        gbar();
+        if (tid == 0)
+            sh[0] = read_status(res) == 0;
+        gbar();
+        return sh[0] != 0;
     }
 
     // Cluster barrier; true iff no CTA had seen an error when it arrived.
@@ -538,18 +599,18 @@ struct ClusterTeam {
         if (size == 1)
             return block_ok();
         const uint32_t ph = phase & 1u;
-        __syncthreads();
-        if (threadIdx.x == 0)
+        gbar();
+        if (tid == 0)
             cs->ok[ph] = read_status(res) == 0 ? 1u : 0u;
         cluster_arrive();
         cluster_wait();
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             uint32_t a = 1;
             for (uint32_t r = 0; r < size; ++r)
                 a &= peer(r)->ok[ph];
             cs->all_ok = a;
         }
-        __syncthreads();
+        gbar();
         ++phase;
         return cs->all_ok != 0;
     }
@@ -561,10 +622,10 @@ struct ClusterTeam {
     __device__ bool gate_wait(LevelState& st)
     {
         const uint32_t ph = phase & 1u;
-        __syncthreads();
+        gbar();
         cluster_arrive();
         cluster_wait();
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             const ClusterShared* p0 = peer(0);
             cs->st[0] = p0->st[0];
             cs->st[1] = p0->st[1];
@@ -574,7 +635,7 @@ struct ClusterTeam {
             cs->st[5] = p0->st[5];
             cs->all_ok = p0->ok[ph];
         }
-        __syncthreads();
+        gbar();
         ++phase;
         st.a = cs->st[0];
         st.b = cs->st[1];
@@ -589,8 +650,8 @@ struct ClusterTeam {
     __device__ bool gate_open(const LevelState& st, bool ok)
     {
         const uint32_t ph = phase & 1u;
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        gbar();
+        if (tid == 0) {
             cs->st[0] = st.a;
             cs->st[1] = st.b;
             cs->st[2] = st.Ka;
@@ -610,8 +671,8 @@ struct ClusterTeam {
     __device__ __forceinline__ void ag_publish(uint32_t cnt, uint32_t esum, uint32_t, unsigned long long*)
     {
         const uint32_t ph = phase & 1u;
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        gbar();
+        if (tid == 0) {
             cs->ag[ph][0] = cnt;
             cs->ag[ph][1] = esum;
             cs->ok[ph] = read_status(res) == 0 ? 1u : 0u;
@@ -625,12 +686,12 @@ struct ClusterTeam {
     {
         const uint32_t ph = phase & 1u;
         cluster_wait();
-        const uint32_t t = threadIdx.x;
+        const uint32_t t = tid;
         pre = 0;
         all = 0;
         if (t == 0)
             cs->all_ok = 1;
-        __syncthreads();
+        gbar();
         for (uint32_t i = t; i < size; i += B) {
             const ClusterShared* pi = peer(i);
             const unsigned long long v = (pi->ag[ph][1] << 32) | (pi->ag[ph][0] & 0xFFFFFFFFull);
@@ -647,7 +708,7 @@ struct ClusterTeam {
 };
 
 // ---------------------------------------------------------------------------
-// Shared memory of one CTA.
+// Shared memory of one thread group (one engine instance).
 // ---------------------------------------------------------------------------
 template <int B, int EMAX>
 struct Smem {
@@ -677,7 +738,18 @@ struct Smem {
     // chunk scalars
     uint32_t m, Ec, Q, Qdeg, hub, npre;
     uint32_t bcast[8];
+    int gsh[kTeamShared];  // the team's group-shared slots (Team::sh)
 };
+
+// Wires a team to the calling thread group (B threads) and its shared memory.
+template <int B, int EMAX, class TeamT>
+__device__ __forceinline__ void bind_group(TeamT& tm, Smem<B, EMAX>& s)
+{
+    tm.tid = gtid<B>();
+    tm.bar = gbar_id<B>();
+    tm.nthr = B;
+    tm.sh = s.gsh;
+}
 
 // Counts of one collected unit (chunk or hub).
 struct Agg {
@@ -695,7 +767,7 @@ struct Chunk {
     Smem<B, EMAX>& s;
     const MatrixView& M;
     uint32_t base;  // key of the pass: edge id e has key base - 1 - e
-    // queue record of position pf_base + threadIdx.x, loaded by the previous
+    // queue record of position pf_base + (group thread), loaded by the previous
     // form() for the chunk that follows it (its latency hides behind that
     // chunk's work); pf_base == kUnvisited: none
     uint32_t pf_base = kUnvisited;
@@ -707,7 +779,7 @@ struct Chunk {
     // parents consumed (the hub counts as 1).
     __device__ uint32_t form(uint32_t p, uint32_t pend)
     {
-        const uint32_t t = threadIdx.x;
+        const uint32_t t = gtid<B>();
         uint32_t deg = 0;
         const bool have = p + t < pend;
         if (have) {
@@ -727,7 +799,7 @@ struct Chunk {
         const uint32_t incl = excl + deg;
         // incl is monotone in t, so the fitting parents are a prefix
         const int fits = have && incl <= (uint32_t)EMAX;
-        const int m = __syncthreads_count(fits);
+        const int m = gsync_count<B>(fits);
         if (fits)
             s.soff[t] = excl;
         if (m > 0 && t == (uint32_t)(m - 1))
@@ -747,10 +819,10 @@ struct Chunk {
             if (nb + t < pend && PB_CHECK(M.res, nb + t < M.n, 109))
                 pf = __ldcg(reinterpret_cast<const uint4*>(M.rec) + nb + t);
         }
-        __syncthreads();
+        gsync<B>();
         if (t == 0)
             s.Ec = m > 0 ? s.soff[m] : 0;
-        __syncthreads();
+        gsync<B>();
         return used;
     }
 
@@ -760,7 +832,7 @@ struct Chunk {
     // with.
     __device__ void form_from_children(uint32_t K0prev)
     {
-        const uint32_t t = threadIdx.x;
+        const uint32_t t = gtid<B>();
         const uint32_t F = s.Q, E = s.Qdeg;
         if (t < F) {
             const uint32_t x = s.so_idx[t];
@@ -777,7 +849,7 @@ struct Chunk {
             s.Ec = E;
             s.hub = 0;
         }
-        __syncthreads();
+        gsync<B>();
     }
 
     // Finds the child edges of the chunk, compacts them, ranks every
@@ -785,7 +857,7 @@ struct Chunk {
     // computes the edge offsets of the ranked children.
     __device__ Agg collect(bool sorted, bool from_pre = false)
     {
-        const uint32_t t = threadIdx.x;
+        const uint32_t t = gtid<B>();
         const uint32_t m = s.m, Ec = s.Ec;
         const uint32_t ept = (Ec + B - 1) / B;
         const uint32_t e0 = t * ept;
@@ -856,7 +928,7 @@ struct Chunk {
                 }
             }
         }
-        __syncthreads();
+        gsync<B>();
         // rank every child inside its parent's run
         for (uint32_t x = t; x < Q; x += B) {
             const uint32_t jp = s.ch_par[x];
@@ -872,7 +944,7 @@ struct Chunk {
             }
             s.so_idx[st + rank] = x;
         }
-        __syncthreads();
+        gsync<B>();
         // edge offsets in ranked order (blocked exclusive scan)
         const uint32_t per = (Q + B - 1) / B;
         const uint32_t i0 = min(t * per, Q), i1 = min(i0 + per, Q);
@@ -891,7 +963,7 @@ struct Chunk {
             s.Qdeg = Qdeg;
             s.npre = 0;
         }
-        __syncthreads();
+        gsync<B>();
         return Agg{Q, Qdeg};
     }
 
@@ -917,7 +989,7 @@ struct Chunk {
     {
         const uint32_t Qdeg = s.Qdeg;
         const uint32_t per = (Qdeg + B - 1) / B;
-        const uint32_t f0 = threadIdx.x * per, f1 = min(f0 + per, Qdeg);
+        const uint32_t f0 = gtid<B>() * per, f1 = min(f0 + per, Qdeg);
         if (f0 >= f1)
             return;
         uint32_t lo = child_of(f0);
@@ -944,17 +1016,17 @@ struct Chunk {
         for_child_edges([&](uint32_t f, uint32_t idx) {
             s.pre[f] = PB_CHECK(M.res, idx < M.nnz, 108) ? ld_ro(M.ci + idx) : 0u;
         });
-        __syncthreads();
-        if (threadIdx.x == 0)
+        gsync<B>();
+        if (gtid<B>() == 0)
             s.npre = Qdeg;
-        __syncthreads();
+        gsync<B>();
     }
 
     // Writes the ranked children of the chunk at positions P0.. and edge
     // bases K0.., then claims their edges for the next level.
     __device__ void place_and_claim(uint32_t P0, uint32_t K0, bool write_perm, bool reverse)
     {
-        const uint32_t t = threadIdx.x;
+        const uint32_t t = gtid<B>();
         const uint32_t Q = s.Q, Qdeg = s.Qdeg;
         const bool have_pre = s.npre == Qdeg && Qdeg > 0;
         for (uint32_t i = t; i < Q; i += B) {
@@ -990,7 +1062,7 @@ struct Chunk {
     __device__ void stage_children(uint32_t at, uint32_t eoff0)
     {
         const uint32_t Q = s.Q;
-        for (uint32_t i = threadIdx.x; i < Q; i += B) {
+        for (uint32_t i = gtid<B>(); i < Q; i += B) {
             const uint32_t x = s.so_idx[i];
             if (PB_CHECK(M.res, (uint64_t)at + i < M.nnz, 130))
                 __stcg(reinterpret_cast<uint4*>(M.stage) + at + i,
@@ -1007,7 +1079,7 @@ struct Chunk {
         uint32_t done = 0, kdone = 0;
         while (done < count) {
             const uint32_t cnt = min((uint32_t)EMAX, count - done);
-            for (uint32_t i = threadIdx.x; i < cnt; i += B) {
+            for (uint32_t i = gtid<B>(); i < cnt; i += B) {
                 uint4 r = make_uint4(0u, 0u, 0u, kdone);
                 if (PB_CHECK(M.res, (uint64_t)at + done + i < M.nnz, 131))
                     r = __ldcg(reinterpret_cast<const uint4*>(M.stage) + at + done + i);
@@ -1023,10 +1095,10 @@ struct Chunk {
                     s.npre = 0;
                 }
             }
-            __syncthreads();
+            gsync<B>();
             const uint32_t qdeg = s.Qdeg;
             place_and_claim(P0 + done, K0 + kdone, write_perm, reverse);
-            __syncthreads();
+            gsync<B>();
             done += cnt;
             kdone += qdeg;
         }
@@ -1045,7 +1117,7 @@ struct Chunk {
     // are also left in key1[r0], key1[r0+1] for a later placement.
     __device__ Agg hub_collect(uint32_t r0, bool sorted)
     {
-        const uint32_t t = threadIdx.x;
+        const uint32_t t = gtid<B>();
         const uint32_t rs = s.prs[0], D = s.pdeg[0], eb = s.peb[0];
         if (M.hub == nullptr) {
             set_status(M.res, kErrCheck, 120);
@@ -1116,7 +1188,7 @@ struct Chunk {
             __stcg(hk1() + r0, Q);
             __stcg(hk1() + r0 + 1, (uint32_t)Qdeg);
         }
-        __syncthreads();
+        gsync<B>();
         return Agg{Q, (uint32_t)Qdeg};
     }
 
@@ -1124,13 +1196,13 @@ struct Chunk {
     __device__ void radix_pass(const uint32_t* sk, const uint32_t* sv, uint32_t* dk, uint32_t* dv, uint32_t Q,
                                uint32_t shift)
     {
-        const uint32_t t = threadIdx.x, lane = t & 31, w = t >> 5;
+        const uint32_t t = gtid<B>(), lane = t & 31, w = t >> 5;
         for (uint32_t d = t; d < 256; d += B)
             s.hist[d] = 0;
-        __syncthreads();
+        gsync<B>();
         for (uint32_t i = t; i < Q; i += B)
             atomicAdd(&s.hist[(__ldcg(sk + i) >> shift) & 255u], 1u);
-        __syncthreads();
+        gsync<B>();
         if (t == 0) {
             uint32_t run = 0;
             for (int d = 0; d < 256; ++d) {
@@ -1139,11 +1211,11 @@ struct Chunk {
                 run += h;
             }
         }
-        __syncthreads();
+        gsync<B>();
         for (uint32_t base0 = 0; base0 < Q; base0 += B) {
             for (uint32_t i = t; i < (uint32_t)(Smem<B, EMAX>::W * 256); i += B)
                 s.hcnt[i] = 0;
-            __syncthreads();
+            gsync<B>();
             const uint32_t i = base0 + t;
             const bool act = i < Q;
             uint32_t key = 0, val = 0, dgt = 0;
@@ -1158,7 +1230,7 @@ struct Chunk {
             const bool leader = act && below == 0;
             if (leader)
                 s.hcnt[w * 256 + dgt] = __popc(peers);
-            __syncthreads();
+            gsync<B>();
             if (act) {
                 uint32_t before = 0;
                 for (uint32_t ww = 0; ww < w; ++ww)
@@ -1167,14 +1239,14 @@ struct Chunk {
                 dk[dst] = key;
                 dv[dst] = val;
             }
-            __syncthreads();
+            gsync<B>();
             for (uint32_t d = t; d < 256; d += B) {
                 uint32_t add = 0;
                 for (int ww = 0; ww < Smem<B, EMAX>::W; ++ww)
                     add += s.hcnt[ww * 256 + d];
                 s.hist[d] += add;
             }
-            __syncthreads();
+            gsync<B>();
         }
     }
 
@@ -1183,7 +1255,7 @@ struct Chunk {
     __device__ void hub_place_and_claim(uint32_t r0, uint32_t Q, uint32_t P0, uint32_t K0, bool write_perm,
                                         bool reverse)
     {
-        const uint32_t t = threadIdx.x;
+        const uint32_t t = gtid<B>();
         const uint32_t rs = s.prs[0];
         uint32_t done = 0, kdone = 0;
         while (done < Q) {
@@ -1213,9 +1285,9 @@ struct Chunk {
                 s.Qdeg = tot;
                 s.npre = 0;
             }
-            __syncthreads();
+            gsync<B>();
             place_and_claim(P0 + done, K0 + kdone, write_perm, reverse);
-            __syncthreads();
+            gsync<B>();
             done += cnt;
             kdone += tot;
         }
@@ -1238,7 +1310,7 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, uns
                          uint32_t& wide_f, uint32_t& wide_e)
 {
     Chunk<B, EMAX> ch{s, M, base};
-    const uint32_t t = threadIdx.x;
+    const uint32_t t = gtid<B>();
     const uint32_t G = team.size, R = team.rank;
     const uint32_t n = M.n;
 
@@ -1293,7 +1365,7 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, uns
                         K += g.esum;
                         next_carry = g.cnt > 0 && g.cnt <= (uint32_t)B && g.esum <= (uint32_t)EMAX &&
                                      s.npre == g.esum;
-                        __syncthreads();
+                        gsync<B>();
                     } else {
                         uint32_t p = st.a;
                         while (p < st.b) {
@@ -1315,7 +1387,7 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, uns
                                 next_carry = single && g.cnt > 0 && g.cnt <= (uint32_t)B &&
                                              g.esum <= (uint32_t)EMAX && s.npre == g.esum;
                             }
-                            __syncthreads();
+                            gsync<B>();
                             p += used;
                         }
                     }
@@ -1400,7 +1472,7 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, uns
             my_esum += g.esum;
             ++nunits;
             p += used;
-            __syncthreads();
+            gsync<B>();
         }
         // publish (level-tagged), then prefetch while the others finish
         ++step;
@@ -1448,7 +1520,7 @@ __device__ bool bfs_pass(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, uns
                     P += g.cnt;
                     K += g.esum;
                 }
-                __syncthreads();
+                gsync<B>();
                 p += used;
             }
         }
@@ -1497,7 +1569,7 @@ __device__ __forceinline__ uint32_t next_peripheral_start(const MatrixView& M, u
 template <int B>
 __device__ void init_nodes(const MatrixView& M, uint32_t R, uint32_t G)
 {
-    for (uint64_t v = (uint64_t)R * B + threadIdx.x; v < M.n; v += (uint64_t)G * B) {
+    for (uint64_t v = (uint64_t)R * B + gtid<B>(); v < M.n; v += (uint64_t)G * B) {
         const uint32_t a = ld_ro(M.rp + v), e = ld_ro(M.rp + v + 1);
         __stcg(reinterpret_cast<uint4*>(M.node) + v, make_uint4(0u, a, e - a, 0u));
     }
@@ -1511,7 +1583,7 @@ template <int B, int EMAX, class TeamT>
 __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& team, unsigned long long* agg,
                                const Options& opt)
 {
-    const uint32_t t = threadIdx.x;
+    const uint32_t t = gtid<B>();
     const uint32_t n = M.n;
     const uint32_t G = team.size, R = team.rank;
     uint32_t start = opt.start;
@@ -1523,6 +1595,8 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& tea
             set_status(M.res, kErrArg, 2);
         return;
     }
+    if (R == 0 && t == 0)
+        M.res->t_begin = globaltimer();
     init_nodes<B>(M, R, G);
     if (!team.sync(1))
         return;
@@ -1646,9 +1720,9 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& tea
             }
             if (t == 0)
                 s.bcast[0] = next_peripheral_start(M, opt.outnodes, ls);
-            __syncthreads();
+            gsync<B>();
             next = s.bcast[0];
-            __syncthreads();
+            gsync<B>();
         } else {
             if constexpr (TeamT::kGrid) {
                 // the halves meet in the team's GridSync words st[8..12]
@@ -1763,7 +1837,85 @@ __device__ void reorder_matrix(Smem<B, EMAX>& s, const MatrixView& M, TeamT& tea
         M.res->ecc = ecc;
         M.res->levels = nlevels;
         M.res->placed = placed;
+        M.res->t_end = globaltimer();
     }
+}
+
+// ---------------------------------------------------------------------------
+// CSR check of one matrix by one thread group (the batch kernels; the
+// single-matrix path runs k_validate over the whole GPU instead): rows
+// ordered and inside [0, nnz], every column below n, and the largest valence
+// (decides whether hub scratch is needed) into res->maxdeg.  Coalesced.
+template <int B>
+__device__ void validate_group(const MatrixView& M, uint32_t* red)
+{
+    const uint32_t t = gtid<B>();
+    uint32_t mx = 0;
+    bool bad = false;
+    for (uint32_t i = t; i < M.n; i += B) {
+        const uint32_t a = ld_ro(M.rp + i), b = ld_ro(M.rp + i + 1);
+        if (b < a || b > M.nnz)
+            bad = true;
+        else
+            mx = max(mx, b - a);
+    }
+    if (t == 0 && (ld_ro(M.rp) != 0 || ld_ro(M.rp + M.n) != M.nnz))
+        bad = true;
+    for (uint32_t k = t; k < M.nnz; k += B)
+        if (ld_ro(M.ci + k) >= M.n)
+            bad = true;
+    if (bad)
+        set_status(M.res, kErrArg, 200);
+    mx = block_reduce_max<B, uint32_t>(mx, red);
+    if (t == 0)
+        atomicMax(&M.res->maxdeg, mx);
+    gsync<B>();
+}
+
+// Bounded wait of a thread group for a matrix's CSR to arrive (the word
+// `ready` is written by a host-to-device copy after the CSR's copies).  A
+// wait that runs out posts PBRCM_ERR_TIMEOUT for the matrix.  The word is
+// read with acquire semantics; the CSR's lines are read only afterwards, and
+// no other matrix shares them (every CSR starts on a 128-byte boundary).
+template <int B>
+__device__ void wait_ready(const uint32_t* ready, unsigned long long wait_ns, DevResult* res, int* flag)
+{
+    if (gtid<B>() == 0) {
+        int ok = 1;
+        unsigned long long t0 = 0;
+        uint32_t spins = 0;
+        while (ld_acquire(ready) == 0u) {
+            if ((++spins & 63u) == 0) {
+                const unsigned long long now = globaltimer();
+                if (t0 == 0) {
+                    t0 = now;
+                } else if (now - t0 > wait_ns) {
+                    set_status(res, kErrTimeout, 210);
+                    ok = 0;
+                    break;
+                }
+            }
+            __nanosleep(spins > 4096 ? 1024 : 128);
+        }
+        *flag = ok;
+    }
+    gsync<B>();
+}
+
+// ---------------------------------------------------------------------------
+// Early exits shared by the reorder kernels.  Returns true if the matrix must
+// not be processed.  Every CTA reads the same values, so all agree.
+template <int EMAX>
+__device__ __forceinline__ bool skip_matrix(const MatrixView& M, bool first_thread)
+{
+    if (read_status(M.res) != 0)
+        return true;
+    if (__ldcg(&M.res->maxdeg) > (uint32_t)EMAX && M.hub == nullptr) {
+        if (first_thread)
+            set_status(M.res, kNeedHub, 0);
+        return true;
+    }
+    return false;
 }
 
 }  // namespace pbrcm

@@ -8,11 +8,9 @@
 //                     (agg: 2 words per CTA for the level all-gather, then
 //                     one barrier flag word per CTA + phantom; all zeroed
 //                     before the launch together with the GridSync words).
-//   k_reorder_batch   many matrices in one cooperative launch: a work list of
-//                     (job, team rank) slots handed out by an atomic counter,
-//                     biggest jobs first; small matrices run on one CTA, big
-//                     ones on a team of CTAs with their own barrier words.
-//   k_bandwidth_*     bandwidth / profile of a caller permutation.
+//   k_bw_*            bandwidth / profile of a caller permutation.
+// The batch kernels (k_reorder_batch, k_reorder_cluster) are in pool.cuh,
+// one translation unit per pool shape (pool_p0.cu .. pool_p4.cu).
 #include <algorithm>
 #include <cstdio>
 
@@ -64,31 +62,6 @@ __global__ void __launch_bounds__(256) k_validate(const uint32_t* __restrict__ r
                  (uint64_t)gridDim.x * blockDim.x);
 }
 
-// one CTA per matrix
-__global__ void __launch_bounds__(256) k_validate_batch(const BatchJob* jobs, uint32_t njobs)
-{
-    for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
-        const MatrixView M = jobs[j].M;
-        validate_one(M.rp, M.ci, M.n, M.nnz, M.res, threadIdx.x, blockDim.x);
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Early exits shared by the reorder kernels.  Returns true if the matrix must
-// not be processed.  Every CTA reads the same values, so all agree.
-template <int EMAX>
-__device__ __forceinline__ bool skip_matrix(const MatrixView& M, bool first_thread)
-{
-    if (read_status(M.res) != 0)
-        return true;
-    if (M.res->maxdeg > (uint32_t)EMAX && M.hub == nullptr) {
-        if (first_thread)
-            set_status(M.res, kNeedHub, 0);
-        return true;
-    }
-    return false;
-}
 
 template <int B, int EMAX>
 __global__ void __launch_bounds__(B, 1) k_reorder_team(MatrixView M, Options opt, GridSync* gs,
@@ -109,46 +82,8 @@ __global__ void __launch_bounds__(B, 1) k_reorder_team(MatrixView M, Options opt
     team.epoch = 0;
     team.wait_ns = opt.wait_ns;
     team.res = M.res;
+    bind_group<B>(team, s);
     reorder_matrix<B, EMAX>(s, M, team, agg, opt);
-}
-
-// Many matrices in one launch.  Every CTA takes the next slot of the work
-// list; a slot names a job and this CTA's rank in the job's team.  Teams are
-// formed from consecutive slots, biggest jobs first; the launch is
-// cooperative, so every CTA is resident and a team's members that joined
-// first only wait (bounded) for the next CTAs that free up.
-template <int B, int EMAX>
-__global__ void __launch_bounds__(B) k_reorder_batch(const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots,
-                                                     uint32_t* counter, Options opt)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto& s = *reinterpret_cast<Smem<B, EMAX>*>(smem_raw);
-    while (true) {
-        if (threadIdx.x == 0)
-            s.bcast[7] = atomicAdd(counter, 1u);
-        __syncthreads();
-        const uint32_t slot = s.bcast[7];
-        __syncthreads();
-        if (slot >= nslots)
-            break;
-        const BatchSlot sl = slots[slot];
-        const BatchJob job = jobs[sl.job];
-        if (skip_matrix<EMAX>(job.M, sl.rank == 0 && threadIdx.x == 0))
-            continue;
-        Team team;
-        team.gs = job.team > 1 ? job.gs : nullptr;
-        team.flags = job.team > 1 ? reinterpret_cast<unsigned int*>(job.words + 2 * job.team) : nullptr;
-        team.size = job.team;
-        team.rank = sl.rank;
-        team.expected = job.team;
-        team.mode = 0;
-        team.target = 0;
-        team.epoch = 0;
-        team.wait_ns = opt.wait_ns;
-        team.res = job.M.res;
-        reorder_matrix<B, EMAX>(s, job.M, team, job.words, opt);
-        __syncthreads();
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -202,143 +137,20 @@ __global__ void __launch_bounds__(256) k_bw_rows(const uint32_t* __restrict__ rp
     }
 }
 
-// A batch launched in thread-block clusters.  First the big matrices,
-// jobs[0..nbig), one per cluster at a time: the cluster's CTA 0 takes the next
-// index from counters[0], the others read it from CTA 0's shared memory, and
-// the cluster reorders the matrix as one ClusterTeam (copt).  Every CTA
-// passes every cluster barrier: the job index and the skip test are the same
-// in all of them, and reorder_matrix stops only through cluster-wide
-// decisions.  When no big matrix is left, every CTA takes the remaining
-// one-CTA slots on its own from counters[1], as k_reorder_batch does.
-template <int B, int EMAX>
-__global__ void __launch_bounds__(B) k_reorder_cluster(const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots,
-                                                       uint32_t nslots, uint32_t* counters, Options copt,
-                                                       Options opt)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto& s = *reinterpret_cast<Smem<B, EMAX>*>(smem_raw);
-    __shared__ ClusterShared cs;
-    __shared__ uint32_t s_job;
-    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
-    const uint32_t csize = cl.num_blocks(), crank = cl.block_rank();
-    while (true) {
-        if (crank == 0 && threadIdx.x == 0)
-            cs.job = atomicAdd(counters, 1u);
-        cluster_arrive();
-        cluster_wait();
-        if (threadIdx.x == 0)
-            s_job = cl.map_shared_rank(&cs, 0)->job;
-        __syncthreads();
-        const uint32_t j = s_job;
-        // nobody goes on while a peer still reads its shared memory
-        cluster_arrive();
-        cluster_wait();
-        if (j >= nbig)
-            break;
-        const BatchJob job = jobs[j];
-        if (!skip_matrix<EMAX>(job.M, crank == 0 && threadIdx.x == 0)) {
-            ClusterTeam team{&cs, csize, crank, 0u, job.M.res};
-            reorder_matrix<B, EMAX>(s, job.M, team, nullptr, copt);
-        }
-        cluster_arrive();
-        cluster_wait();
-    }
-    // one-CTA jobs: no cluster barrier and no shared-memory access across CTAs
-    // from here on
-    while (true) {
-        if (threadIdx.x == 0)
-            s.bcast[7] = atomicAdd(counters + 1, 1u);
-        __syncthreads();
-        const uint32_t slot = s.bcast[7];
-        __syncthreads();
-        if (slot >= nslots)
-            break;
-        const BatchSlot sl = slots[slot];
-        const BatchJob job = jobs[sl.job];
-        if (skip_matrix<EMAX>(job.M, threadIdx.x == 0))
-            continue;
-        Team team;
-        team.gs = nullptr;
-        team.flags = nullptr;
-        team.size = 1;
-        team.rank = 0;
-        team.expected = 1;
-        team.mode = 0;
-        team.target = 0;
-        team.epoch = 0;
-        team.wait_ns = opt.wait_ns;
-        team.res = job.M.res;
-        reorder_matrix<B, EMAX>(s, job.M, team, job.words, opt);
-        __syncthreads();
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 namespace {
 
+// The one-matrix team kernel of one shape.
 template <int B, int EMAX>
 struct Variant {
     static size_t smem() { return sizeof(Smem<B, EMAX>); }
     static cudaError_t prepare()
     {
-        static cudaError_t once = [] {
-            cudaError_t e = cudaFuncSetAttribute(k_reorder_team<B, EMAX>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
-            if (e != cudaSuccess)
-                return e;
-            e = cudaFuncSetAttribute(k_reorder_batch<B, EMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem());
-            if (e != cudaSuccess)
-                return e;
-            e = cudaFuncSetAttribute(k_reorder_cluster<B, EMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem());
-            if (e != cudaSuccess)
-                return e;
-            return cudaFuncSetAttribute(k_reorder_cluster<B, EMAX>, cudaFuncAttributeNonPortableClusterSizeAllowed,
-                                        1);
-        }();
+        static cudaError_t once = cudaFuncSetAttribute(k_reorder_team<B, EMAX>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
         return once;
-    }
-    static cudaLaunchConfig_t cluster_config(int csize, int nclusters, cudaStream_t st, cudaLaunchAttribute* at)
-    {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(csize * nclusters));
-        cfg.blockDim = dim3(B);
-        cfg.dynamicSmemBytes = smem();
-        cfg.stream = st;
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = (unsigned)csize;
-        at[0].val.clusterDim.y = 1;
-        at[0].val.clusterDim.z = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        return cfg;
-    }
-    static int cluster_max_active(int csize)
-    {
-        if (prepare() != cudaSuccess)
-            return 0;
-        cudaLaunchAttribute at[1];
-        cudaLaunchConfig_t cfg = cluster_config(csize, 1, nullptr, at);
-        int n = 0;
-        if (cudaOccupancyMaxActiveClusters(&n, (void*)k_reorder_cluster<B, EMAX>, &cfg) != cudaSuccess) {
-            cudaGetLastError();
-            return 0;
-        }
-        return n;
-    }
-    static cudaError_t cluster(const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots, uint32_t nslots,
-                               uint32_t* counters, const Options& copt, const Options& opt, int csize, int nclusters,
-                               cudaStream_t st)
-    {
-        cudaError_t e = prepare();
-        if (e != cudaSuccess)
-            return e;
-        cudaLaunchAttribute at[1];
-        cudaLaunchConfig_t cfg = cluster_config(csize, nclusters, st, at);
-        return cudaLaunchKernelEx(&cfg, k_reorder_cluster<B, EMAX>, jobs, nbig, slots, nslots, counters, copt, opt);
     }
     static int team_max_ctas(int sms)
     {
@@ -346,16 +158,6 @@ struct Variant {
             return 0;
         int nb = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_reorder_team<B, EMAX>, B, smem()) != cudaSuccess)
-            return 0;
-        return nb * sms;
-    }
-    static int batch_max_ctas(int sms)
-    {
-        if (prepare() != cudaSuccess)
-            return 0;
-        int nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_reorder_batch<B, EMAX>, B, smem()) !=
-            cudaSuccess)
             return 0;
         return nb * sms;
     }
@@ -371,26 +173,6 @@ struct Variant {
         return cudaLaunchCooperativeKernel((const void*)k_reorder_team<B, EMAX>, dim3(ctas), dim3(B), args, smem(),
                                            st);
     }
-    static cudaError_t batch(const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
-                             const Options& opt, int ctas, bool cooperative, cudaStream_t st)
-    {
-        cudaError_t e = prepare();
-        if (e != cudaSuccess)
-            return e;
-        if (!cooperative) {
-            // no team: CTAs never wait for each other, a plain launch will do
-            k_reorder_batch<B, EMAX><<<ctas, B, smem(), st>>>(jobs, slots, nslots, counter, opt);
-            return cudaGetLastError();
-        }
-        const BatchJob* j = jobs;
-        const BatchSlot* sl = slots;
-        uint32_t ns = nslots;
-        uint32_t* c = counter;
-        Options o = opt;
-        void* args[] = {&j, &sl, &ns, &c, &o};
-        return cudaLaunchCooperativeKernel((const void*)k_reorder_batch<B, EMAX>, dim3(ctas), dim3(B), args, smem(),
-                                           st);
-    }
 };
 
 }  // namespace
@@ -401,6 +183,14 @@ const VariantInfo kVariants[kNumVariants] = {
     {512, 2048},
 };
 
+const PoolInfo kPools[kNumPools] = {
+    {512, 2048, 512, 2048},
+    {512, 2048, 256, 1024},
+    {512, 2048, 128, 512},
+    {512, 2048, 64, 256},
+    {128, 512, 128, 512},
+};
+
 #define PBRCM_DISPATCH(v, CALL)                     \
     switch (v) {                                    \
     case 0: return Variant<128, 512>::CALL;         \
@@ -409,10 +199,18 @@ const VariantInfo kVariants[kNumVariants] = {
     default: break;                                 \
     }
 
+// the pool shapes' entry points (pool_p<N>.cu, one translation unit each)
+extern const PoolFns kPoolFns0, kPoolFns1, kPoolFns2, kPoolFns3, kPoolFns4;
+static const PoolFns* const kPoolTable[kNumPools] = {&kPoolFns0, &kPoolFns1, &kPoolFns2, &kPoolFns3, &kPoolFns4};
+
 size_t variant_smem(int v)
 {
-    PBRCM_DISPATCH(v, smem());
-    return 0;
+    switch (v) {
+    case 0: return sizeof(Smem<128, 512>);
+    case 1: return sizeof(Smem<256, 1024>);
+    case 2: return sizeof(Smem<512, 2048>);
+    default: return 0;
+    }
 }
 
 int team_max_ctas(int v, int sms)
@@ -421,10 +219,9 @@ int team_max_ctas(int v, int sms)
     return 0;
 }
 
-int batch_max_ctas(int v, int sms)
+int batch_max_ctas(int p, int sms)
 {
-    PBRCM_DISPATCH(v, batch_max_ctas(sms));
-    return 0;
+    return p >= 0 && p < kNumPools ? kPoolTable[p]->batch_max_ctas(sms) : 0;
 }
 
 cudaError_t launch_team(int v, const MatrixView& M, const Options& opt, GridSync* gs, unsigned long long* agg,
@@ -434,25 +231,26 @@ cudaError_t launch_team(int v, const MatrixView& M, const Options& opt, GridSync
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_batch(int v, const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
+cudaError_t launch_batch(int p, const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
                          const Options& opt, int ctas, bool cooperative, cudaStream_t st)
 {
-    PBRCM_DISPATCH(v, batch(jobs, slots, nslots, counter, opt, ctas, cooperative, st));
-    return cudaErrorInvalidValue;
+    if (p < 0 || p >= kNumPools)
+        return cudaErrorInvalidValue;
+    return kPoolTable[p]->batch(jobs, slots, nslots, counter, opt, ctas, cooperative, st);
 }
 
-int cluster_max_active(int v, int csize)
+int cluster_max_active(int p, int csize)
 {
-    PBRCM_DISPATCH(v, cluster_max_active(csize));
-    return 0;
+    return p >= 0 && p < kNumPools ? kPoolTable[p]->cluster_max_active(csize) : 0;
 }
 
-cudaError_t launch_cluster(int v, const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots, uint32_t nslots,
+cudaError_t launch_cluster(int p, const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots, uint32_t nslots,
                            uint32_t* counters, const Options& copt, const Options& opt, int csize, int nclusters,
                            cudaStream_t st)
 {
-    PBRCM_DISPATCH(v, cluster(jobs, nbig, slots, nslots, counters, copt, opt, csize, nclusters, st));
-    return cudaErrorInvalidValue;
+    if (p < 0 || p >= kNumPools)
+        return cudaErrorInvalidValue;
+    return kPoolTable[p]->cluster(jobs, nbig, slots, nslots, counters, copt, opt, csize, nclusters, st);
 }
 
 cudaError_t launch_validate(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint32_t nnz, DevResult* res,
@@ -466,14 +264,6 @@ cudaError_t launch_validate(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_validate_batch(const BatchJob* jobs, uint32_t njobs, int sms, cudaStream_t st)
-{
-    int blocks = (int)std::min<uint32_t>(njobs, (uint32_t)sms * 8);
-    if (blocks < 1)
-        blocks = 1;
-    k_validate_batch<<<blocks, 256, 0, st>>>(jobs, njobs);
-    return cudaGetLastError();
-}
 
 void launch_perm_inverse(const uint32_t* perm, uint32_t n, uint32_t* inv, DevResult* res, int blocks,
                          cudaStream_t st)

@@ -18,23 +18,46 @@ struct VariantInfo {
 constexpr int kNumVariants = 3;
 extern const VariantInfo kVariants[kNumVariants];
 
+// Shapes of the batch kernels ("pools"): CTAs of `block` threads (a
+// cluster team of whole CTAs chunks `emax` edges per CTA) split into groups
+// of `group` threads that reorder one matrix each (`gemax` edges per chunk).
+struct PoolInfo {
+    int block;
+    int emax;
+    int group;
+    int gemax;
+};
+constexpr int kNumPools = 5;
+extern const PoolInfo kPools[kNumPools];
+
+// Entry points of one pool shape (see launch_batch / launch_cluster).
+struct PoolFns {
+    int (*batch_max_ctas)(int sms);
+    int (*cluster_max_active)(int csize);
+    cudaError_t (*batch)(const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
+                         const Options& opt, int ctas, bool cooperative, cudaStream_t st);
+    cudaError_t (*cluster)(const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots, uint32_t nslots,
+                           uint32_t* counters, const Options& copt, const Options& opt, int csize, int nclusters,
+                           cudaStream_t st);
+};
+
 size_t variant_smem(int v);
 int team_max_ctas(int v, int sms);   // co-resident CTAs of the team kernel
-int batch_max_ctas(int v, int sms);  // co-resident CTAs of the batch kernel
+int batch_max_ctas(int p, int sms);  // co-resident CTAs of pool p's batch kernel
 
 cudaError_t launch_validate(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint32_t nnz, DevResult* res,
                             int sms, cudaStream_t st);
-cudaError_t launch_validate_batch(const BatchJob* jobs, uint32_t njobs, int sms, cudaStream_t st);
 cudaError_t launch_team(int v, const MatrixView& M, const Options& opt, GridSync* gs, unsigned long long* agg,
                         int ctas, cudaStream_t st);
-// cooperative: required when some job has a team of more than one CTA
-cudaError_t launch_batch(int v, const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
+// pool p's batch kernel; cooperative: required when some job has a team of
+// more than one group
+cudaError_t launch_batch(int p, const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
                          const Options& opt, int ctas, bool cooperative, cudaStream_t st);
 // A batch in thread-block clusters: jobs[0..nbig) one per cluster (team
-// options copt), then the one-CTA slots by single CTAs (opt); counters[0..1]
-// zeroed per launch.
-int cluster_max_active(int v, int csize);  // co-resident clusters of that size
-cudaError_t launch_cluster(int v, const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots, uint32_t nslots,
+// options copt), then the one-group slots by pool p's groups (opt);
+// counters[0..1] zeroed per launch.
+int cluster_max_active(int p, int csize);  // co-resident clusters of that size
+cudaError_t launch_cluster(int p, const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots, uint32_t nslots,
                            uint32_t* counters, const Options& copt, const Options& opt, int csize, int nclusters,
                            cudaStream_t st);
 // inv[perm[k]] = k over a zeroed-to-0xFF inv; a non-permutation posts

@@ -23,7 +23,17 @@
 // Set-up: the first call on a device, with that device current, looks up the
 // array's device address (cudaGetSymbolAddress; in host code the array's
 // name is only a host-side stand-in) and the launch shape; that first call
-// should come before any stream capture.
+// should come before any stream capture.  The looked-up address belongs to
+// the device's current context: after a cudaDeviceReset the process must not
+// call this entry point again.
+//
+// Engine: the one-matrix team kernel without the parts that need more
+// scratch -- no speculative final pass beside the start search (second
+// queue-record array), no staging of multi-chunk levels (2 nnz records) and
+// no hub path (rows over kNoAllocMaxValence are refused) -- so it is slower
+// than pbrcm_reorder_device on matrices with wide levels; same result.
+// result->device_ms is the reorder kernel's time from the engine's own
+// %globaltimer stamps.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -84,6 +94,7 @@ __global__ void __launch_bounds__(kNoAllocB, 1) k_reorder_team_noalloc(MatrixVie
     team.epoch = 0;
     team.wait_ns = opt.wait_ns;
     team.res = M.res;
+    bind_group<kNoAllocB>(team, s);
     reorder_matrix<kNoAllocB, kNoAllocEmax>(s, M, team, words, opt);
 }
 
@@ -98,7 +109,8 @@ struct DeviceSetup {
 std::mutex g_setup_mu;
 DeviceSetup g_setup[64];
 
-// Once per device, with that device current.
+// Once per device, with that device current.  A set-up that fails is not
+// kept: the next call tries again.
 int32_t setup_device(int dev, DeviceSetup*& out)
 {
     if (dev < 0 || dev >= 64)
@@ -106,7 +118,7 @@ int32_t setup_device(int dev, DeviceSetup*& out)
     std::lock_guard<std::mutex> lk(g_setup_mu);
     DeviceSetup& d = g_setup[dev];
     if (!d.ready) {
-        d.ready = true;
+        d.rc = PBRCM_OK;
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) {
             d.rc = PBRCM_ERR_CUDA;
@@ -126,6 +138,9 @@ int32_t setup_device(int dev, DeviceSetup*& out)
                 d.ctas = std::min(std::min(nb * d.sms, d.sms), kNoAllocMaxCtas);
             }
         }
+        if (d.rc != PBRCM_OK)
+            cudaGetLastError();  // clear the failed call's error for the caller
+        d.ready = d.rc == PBRCM_OK;
     }
     out = &d;
     return d.rc;
@@ -186,7 +201,8 @@ extern "C" int32_t pbrcm_reorder_device_noalloc(const uint32_t* d_row_ptr, const
         return PBRCM_ERR_CUDA;
     fill_result(h, opt, result);
     if (result) {
-        result->device_ms = 0.f;
+        // the engine's own %globaltimer stamps (no event to create)
+        result->device_ms = h.t_end > h.t_begin ? (float)((h.t_end - h.t_begin) * 1e-6) : 0.f;
         result->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     return map_status(h.status);

@@ -94,6 +94,7 @@ struct Request {
     bool team = false;
     bool cluster = false;  // team as one thread-block cluster (no hub row)
     int ctas = 1;       // CTAs of its launch (team size, or 1)
+    int units = 1;      // share of the GPU it holds (see pbrcm_session::units_per_sm)
     int stream = 0;
     cudaEvent_t ev = nullptr;
     int state = 0;  // 0 queued, 1 running, 2 done
@@ -109,11 +110,14 @@ struct pbrcm_session {
     uint32_t max_inflight = 0;
     std::vector<cudaStream_t> streams;
     std::vector<int> stream_busy;  // requests in flight per stream
-    int small_variant = 1;
+    int small_pool = 0;            // shape of one-CTA requests (kPools 0: one 512-thread group; 4: 128 threads)
     uint32_t team_cutoff_n = 1u << 18;
     int max_ctas = 0;              // largest team (co-resident CTAs of the team kernel)
-    int cap_ctas = 0;              // CTAs the running requests may hold together
-    int ctas_in_use = 0;
+    // GPU share in units: an SM holds units_per_sm one-CTA requests, or one
+    // CTA of a team (which takes a whole SM)
+    int units_per_sm = 1;
+    int cap_ctas = 0;              // units the running requests may hold together
+    int ctas_in_use = 0;           // units held
     int team_min = 4, team_max = 64;
     int idle_team = 0;             // team of a large request that finds the GPU idle (0 = no boost)
     // largest cluster team (0: cooperative teams only).  Off by default: on
@@ -215,20 +219,23 @@ bool pbrcm_session::launch(Request* r)
     ok = ok && cudaMemsetAsync(d_counter, 0, 16, st) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(d_job, r->host + r->off_view, sizeof(BatchJob) + sizeof(BatchSlot),
                                cudaMemcpyHostToDevice, st) == cudaSuccess;
-    ok = ok && launch_validate(M.rp, M.ci, M.n, M.nnz, M.res, c.sms, st) == cudaSuccess;
+    // the batch and cluster kernels check the CSR themselves; the team
+    // kernel needs the separate check first
+    if (r->team && !r->cluster)
+        ok = ok && launch_validate(M.rp, M.ci, M.n, M.nnz, M.res, c.sms, st) == cudaSuccess;
     if (r->cluster) {
         // one thread-block cluster: no cooperative launch, so it runs beside
         // the other requests' kernels
         Options copt = r->opt;
         copt.solo_parents = c.cluster_solo_parents;
         copt.solo_edges = c.cluster_solo_edges;
-        ok = ok && launch_cluster(small_variant, d_job, 1, d_slot, 0, d_counter, copt, r->opt, r->ctas, 1, st) ==
+        ok = ok && launch_cluster(small_pool, d_job, 1, d_slot, 0, d_counter, copt, r->opt, r->ctas, 1, st) ==
                        cudaSuccess;
     } else if (r->team)
         ok = ok && launch_team(c.team_variant, M, r->opt, reinterpret_cast<GridSync*>(D + r->d_gs),
                                reinterpret_cast<unsigned long long*>(D + r->d_agg), r->ctas, st) == cudaSuccess;
     else
-        ok = ok && launch_batch(small_variant, d_job, d_slot, 1, d_counter, r->opt, 1, false, st) == cudaSuccess;
+        ok = ok && launch_batch(small_pool, d_job, d_slot, 1, d_counter, r->opt, 1, false, st) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(r->host + r->off_perm, M.perm, 4 * (size_t)r->n, cudaMemcpyDeviceToHost, st) ==
                    cudaSuccess;
     ok = ok && cudaMemcpyAsync(r->host + r->off_res, M.res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) ==
@@ -246,7 +253,7 @@ void pbrcm_session::retire(Request* r)
     r->state = 2;
     r->t_done = Clock::now();
     bytes_in_flight -= r->dev_bytes;
-    ctas_in_use -= r->ctas;
+    ctas_in_use -= r->units;
     stream_busy[r->stream] -= 1;
     ++completed;
     lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
@@ -300,7 +307,8 @@ void pbrcm_session::run()
             if (bytes_in_flight + r->dev_bytes > cap_bytes && !running.empty())
                 break;
             const int need = choose_ctas(r);
-            if (ctas_in_use + need > cap_ctas && !running.empty())
+            const int units = r->team && !r->cluster ? need * units_per_sm : need;
+            if (ctas_in_use + units > cap_ctas && !running.empty())
                 break;
             int free_stream = -1;
             for (size_t k = 0; k < stream_busy.size(); ++k)
@@ -313,8 +321,9 @@ void pbrcm_session::run()
             queued.pop_front();
             r->stream = free_stream;
             r->ctas = need;
+            r->units = units;
             stream_busy[free_stream] += 1;
-            ctas_in_use += need;
+            ctas_in_use += units;
             bytes_in_flight += r->dev_bytes;
             peak_bytes = std::max(peak_bytes, bytes_in_flight);
             r->state = 1;
@@ -323,7 +332,7 @@ void pbrcm_session::run()
                 r->state = 2;
                 r->t_done = Clock::now();
                 bytes_in_flight -= r->dev_bytes;
-                ctas_in_use -= need;
+                ctas_in_use -= units;
                 stream_busy[free_stream] -= 1;
                 ++completed;
             } else {
@@ -366,9 +375,11 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
         }
         s->streams.push_back(st);
     }
-    s->small_variant = s->C->batch_variant;
+    s->small_pool = s->C->session_pool;
+    s->team_cutoff_n = s->C->session_cutoff_n;
     s->max_ctas = std::max(1, team_max_ctas(s->C->team_variant, s->C->sms));
-    s->cap_ctas = std::max(1, batch_max_ctas(s->small_variant, s->C->sms));
+    s->cap_ctas = std::max(1, batch_max_ctas(s->small_pool, s->C->sms));
+    s->units_per_sm = std::max(1, s->cap_ctas / std::max(1, s->C->sms));
     s->stream_busy.assign(s->streams.size(), 0);
     if (const char* e = std::getenv("PBRCM_SESSION_TEAM_NNZ"))
         s->team_nnz = std::max<uint64_t>(1, std::strtoull(e, nullptr, 10));
@@ -435,7 +446,7 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     for (uint32_t i = 0; i < n; ++i)
         maxdeg = std::max(maxdeg, row_ptr[i + 1] - row_ptr[i]);
     r->maxdeg = maxdeg;
-    const int emax_small = kVariants[s->small_variant].emax;
+    const int emax_small = kPools[s->small_pool].gemax;
     r->team = n > s->team_cutoff_n || maxdeg > (uint32_t)emax_small;
     r->cluster = r->team && s->cluster_max >= 2 && maxdeg <= (uint32_t)emax_small;
     size_t offs[10];

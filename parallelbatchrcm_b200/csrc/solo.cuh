@@ -1,0 +1,460 @@
+// solo.cuh -- the one-group engine of the batch kernels: the whole reorder of
+// one matrix (start search, Cuthill-McKee pass, reverse, bandwidth) by one
+// thread group, with the visited set in shared memory.
+//
+// What it computes is what engine.cuh computes (the serial stable order of
+// src/rcm_cpu.cpp:57-104 from the start node of
+// src/simple_peripheral.cpp:92-141, and the bandwidth of src/main.cpp:143-184);
+// how differs, because a group that owns its matrix alone needs no claim
+// protocol:
+//
+//   * the queue is walked in chunks of consecutive positions (at most B
+//     parents and EMAX edges, never across a level boundary); a chunk's
+//     children are the still-unvisited neighbours, each taken by the first
+//     (parent, slot) that reaches it -- exactly the serial loop, since every
+//     node an earlier chunk placed is already marked;
+//   * visited is a bitmap in shared memory (n <= kSoloMaxN), so checking a
+//     neighbour costs no global load and marking one no atomic in global
+//     memory; inside a chunk a shared-memory hash keeps the first edge to a
+//     node (atomicMin of the edge index);
+//   * every entry's neighbour record -- its column and that column's row
+//     start and valence -- is one 16-byte record of an edge table built once
+//     per matrix (solo_build_edges, during the CSR check), so a chunk needs
+//     one dependent global load per edge (coalesced along each row) instead
+//     of a column load followed by a node-table load;
+//   * the children of a chunk that is a whole level, if they fit one chunk,
+//     stay in shared memory as the next chunk's parents.
+//
+// Per chunk: the edge-to-parent map, the edge records, the visited test and
+// the hash insert, a warp-ballot compaction in edge order, the rank of each
+// parent's children by (valence, slot), the writes of the queue records and
+// the permutation, and the visited marks -- six group barriers.
+#pragma once
+
+#include "engine.cuh"
+
+namespace pbrcm {
+
+constexpr uint32_t kSoloEmpty = 0xFFFFFFFFu;
+
+// Shared memory of one solo group (B threads, EMAX edges per chunk).
+template <int B, int EMAX>
+struct SoloSmem {
+    static constexpr int W = B / 32;
+    static constexpr int H = 2 * EMAX;  // dedup table slots (power of two, > 2x a chunk's candidates)
+    uint32_t vis[kSoloMaxN / 32];
+    // parents of the chunk
+    uint32_t pn[B], prs[B], pdeg[B];
+    uint32_t soff[B + 1];
+    uint32_t cs[B], cc[B];  // first compacted child / child count per parent
+    uint32_t epar[EMAX];    // chunk edge -> parent
+    uint32_t hkey[H], hval[H];
+    // the chunk's children in edge order, then their ranked order
+    uint32_t ch_c[EMAX], ch_rs[EMAX], ch_deg[EMAX], ch_par[EMAX];
+    uint32_t so_idx[EMAX];
+    uint32_t wcnt[W];
+    uint32_t scanbuf[2][W];
+    uint32_t tmp32[W + 1];
+    unsigned long long tmp64[2 * W + 2];
+    uint32_t m, Ec, Q, Qdeg, carry;
+    uint32_t bcast[4];
+};
+
+template <int B, int EMAX>
+struct Solo {
+    static constexpr int MAXEPT = EMAX / B;
+    static_assert(EMAX % B == 0 && (EMAX & (EMAX - 1)) == 0, "EMAX: a power of two, a multiple of B");
+    SoloSmem<B, EMAX>& s;
+    const MatrixView& M;
+    const uint4* e2;
+
+    __device__ __forceinline__ bool visited(uint32_t c) const { return (s.vis[c >> 5] >> (c & 31)) & 1u; }
+    __device__ __forceinline__ void mark(uint32_t c) { atomicOr(&s.vis[c >> 5], 1u << (c & 31)); }
+
+    // Loads the next chunk's parents from the queue records rec[p .. pend):
+    // the longest prefix of at most B parents with at most EMAX edges (every
+    // row fits one chunk: the engine is only used when the largest valence
+    // is at most EMAX).  Returns the number of parents.
+    __device__ uint32_t form(uint32_t p, uint32_t pend)
+    {
+        const uint32_t t = gtid<B>();
+        uint32_t deg = 0;
+        const bool have = p + t < pend;
+        if (have) {
+            const uint4 r = __ldcg(reinterpret_cast<const uint4*>(M.rec) + p + t);
+            s.pn[t] = r.x;
+            s.prs[t] = r.y;
+            s.pdeg[t] = r.z;
+            deg = r.z;
+        }
+        uint32_t total;
+        const uint32_t excl = block_scan1<B>(deg, total, s.scanbuf[0]);
+        const uint32_t incl = excl + deg;
+        const int fits = have && incl <= (uint32_t)EMAX;
+        const int m = gsync_count<B>(fits);
+        if (fits)
+            s.soff[t] = excl;
+        if (m > 0 && t == (uint32_t)(m - 1)) {
+            s.soff[m] = incl;
+            s.m = (uint32_t)m;
+            s.Ec = incl;
+        }
+        gsync<B>();
+        return (uint32_t)m;
+    }
+
+    // The ranked children of the last chunk become the parents of the next.
+    __device__ void form_from_children()
+    {
+        const uint32_t t = gtid<B>();
+        const uint32_t Q = s.Q;
+        uint32_t deg = 0;
+        if (t < Q) {
+            const uint32_t x = s.so_idx[t];
+            s.pn[t] = s.ch_c[x];
+            s.prs[t] = s.ch_rs[x];
+            s.pdeg[t] = s.ch_deg[x];
+            deg = s.ch_deg[x];
+        }
+        uint32_t total;
+        const uint32_t excl = block_scan1<B>(deg, total, s.scanbuf[1]);
+        if (t < Q)
+            s.soff[t] = excl;
+        if (t == 0) {
+            s.soff[Q] = total;
+            s.m = Q;
+            s.Ec = total;
+        }
+        gsync<B>();
+    }
+
+    // One chunk: finds the children of parents [0, m), ranks them (sorted:
+    // by valence, stable; else slot order), writes their queue records at
+    // positions P.. and, with write_perm, the permutation, and marks them
+    // visited.  Returns the number of children.
+    __device__ uint32_t step(uint32_t P, bool sorted, bool write_perm, bool reverse)
+    {
+        const uint32_t t = gtid<B>(), lane = t & 31u, w = t >> 5;
+        const uint32_t m = s.m, Ec = s.Ec;
+        // edge -> parent map, parent counters, an empty dedup table
+        for (uint32_t j = t; j < m; j += B) {
+            for (uint32_t e = s.soff[j]; e < s.soff[j + 1]; ++e)
+                s.epar[e] = j;
+            s.cs[j] = kSoloEmpty;
+            s.cc[j] = 0;
+        }
+        for (uint32_t i = t; i < (uint32_t)SoloSmem<B, EMAX>::H; i += B) {
+            s.hkey[i] = kSoloEmpty;
+            s.hval[i] = kSoloEmpty;
+        }
+        gsync<B>();
+        // warp w owns edges [w * 32 * MAXEPT, ...); lane l takes e = base +
+        // l + 32 r, so that a warp reads consecutive records of a row
+        const uint32_t base = w * 32u * MAXEPT;
+        uint4 v[MAXEPT];
+        uint32_t slot[MAXEPT];
+        bool cand[MAXEPT];
+#pragma unroll
+        for (int r = 0; r < MAXEPT; ++r) {
+            const uint32_t e = base + lane + 32u * r;
+            cand[r] = false;
+            v[r] = make_uint4(0u, 0u, 0u, 0u);
+            if (e < Ec) {
+                const uint32_t j = s.epar[e];
+                const uint64_t idx = (uint64_t)s.prs[j] + (e - s.soff[j]);
+                if (PB_CHECK(M.res, idx < M.nnz, 601))
+                    v[r] = __ldcg(e2 + idx);
+                cand[r] = PB_CHECK(M.res, v[r].x < M.n, 602) && !visited(v[r].x);
+            }
+        }
+        // first edge to each unvisited node: insert the node into the table
+        // (linear probing; at most EMAX distinct keys in 2 EMAX slots, so a
+        // free slot is always found), keep the smallest edge index
+        constexpr uint32_t mask = (uint32_t)SoloSmem<B, EMAX>::H - 1u;
+#pragma unroll
+        for (int r = 0; r < MAXEPT; ++r) {
+            slot[r] = 0;
+            if (cand[r]) {
+                const uint32_t c = v[r].x;
+                uint32_t h = (c * 2654435761u) & mask;
+                while (true) {
+                    const uint32_t k = atomicCAS(&s.hkey[h], kSoloEmpty, c);
+                    if (k == kSoloEmpty || k == c)
+                        break;
+                    h = (h + 1u) & mask;
+                }
+                slot[r] = h;
+                atomicMin(&s.hval[h], base + lane + 32u * r);
+            }
+        }
+        gsync<B>();
+        // the winners, compacted in edge order: per warp by ballot, then the
+        // warps' counts
+        uint32_t cnt = 0, posr[MAXEPT];
+        bool win[MAXEPT];
+#pragma unroll
+        for (int r = 0; r < MAXEPT; ++r) {
+            win[r] = cand[r] && s.hval[slot[r]] == base + lane + 32u * r;
+            const uint32_t bal = __ballot_sync(kFull, win[r]);
+            posr[r] = cnt + __popc(bal & ((1u << lane) - 1u));
+            cnt += __popc(bal);
+        }
+        if (lane == 0)
+            s.wcnt[w] = cnt;
+        gsync<B>();
+        uint32_t wbase = 0, Q = 0;
+#pragma unroll
+        for (int i = 0; i < SoloSmem<B, EMAX>::W; ++i) {
+            const uint32_t c = s.wcnt[i];
+            wbase += (uint32_t)i < w ? c : 0u;
+            Q += c;
+        }
+#pragma unroll
+        for (int r = 0; r < MAXEPT; ++r) {
+            if (win[r]) {
+                const uint32_t x = wbase + posr[r];
+                const uint32_t j = s.epar[base + lane + 32u * r];
+                s.ch_c[x] = v[r].x;
+                s.ch_rs[x] = v[r].y;
+                s.ch_deg[x] = v[r].z;
+                s.ch_par[x] = j;
+                atomicAdd(&s.cc[j], 1u);
+                atomicMin(&s.cs[j], x);
+            }
+        }
+        gsync<B>();
+        // rank inside each parent's run: (valence, position) when sorted
+        for (uint32_t x = t; x < Q; x += B) {
+            const uint32_t j = s.ch_par[x];
+            const uint32_t st = s.cs[j], len = s.cc[j];
+            uint32_t rank = x - st;
+            if (sorted && len > 1) {
+                const uint32_t dx = s.ch_deg[x];
+                rank = 0;
+                for (uint32_t y = st; y < st + len; ++y) {
+                    const uint32_t dy = s.ch_deg[y];
+                    rank += (dy < dx) || (dy == dx && y < x);
+                }
+            }
+            s.so_idx[st + rank] = x;
+        }
+        gsync<B>();
+        // place: queue records, the permutation, the visited marks
+        uint32_t dsum = 0;
+        for (uint32_t i = t; i < Q; i += B) {
+            const uint32_t x = s.so_idx[i];
+            const uint32_t pos = P + i;
+            if (PB_CHECK(M.res, pos < M.n, 603)) {
+                __stcg(reinterpret_cast<uint4*>(M.rec) + pos, make_uint4(s.ch_c[x], s.ch_rs[x], s.ch_deg[x], 0u));
+                if (write_perm)
+                    M.perm[reverse ? M.n - 1 - pos : pos] = s.ch_c[x];
+            }
+            mark(s.ch_c[x]);
+            dsum += s.ch_deg[x];
+        }
+        dsum = block_reduce_sum<B, uint32_t>(dsum, s.tmp32);  // ends with a group barrier
+        if (t == 0) {
+            s.Q = Q;
+            s.Qdeg = dsum;
+        }
+        gsync<B>();
+        return Q;
+    }
+};
+
+// The per-edge neighbour records of a matrix (e2[k] = (c, rp[c], rp[c+1] -
+// rp[c], 0) for c = ci[k]) by one group, coalesced; columns out of range are
+// left to the CSR check.
+template <int B>
+__device__ void solo_build_edges(const MatrixView& M, uint4* e2)
+{
+    for (uint32_t k = gtid<B>(); k < M.nnz; k += B) {
+        const uint32_t c = ld_ro(M.ci + k);
+        uint4 r = make_uint4(c, 0u, 0u, 0u);
+        if (c < M.n) {
+            const uint32_t a = ld_ro(M.rp + c), b = ld_ro(M.rp + c + 1);
+            r.y = a;
+            r.z = b - a;
+        }
+        __stcg(e2 + k, r);
+    }
+}
+
+// One ordered BFS pass from `start` by one solo group.  Fills rec[0 ..
+// placed); returns the level count and the first position of the last level.
+template <int B, int EMAX>
+__device__ void solo_pass(Solo<B, EMAX>& so, uint32_t start, bool sorted, bool write_perm, bool reverse,
+                          uint32_t& placed, uint32_t& nlevels, uint32_t& last_start)
+{
+    SoloSmem<B, EMAX>& s = so.s;
+    const MatrixView& M = so.M;
+    const uint32_t t = gtid<B>();
+    const uint32_t words = (M.n + 31u) / 32u;
+    for (uint32_t i = t; i < words; i += B)
+        s.vis[i] = 0u;
+    gsync<B>();
+    if (t == 0) {
+        const uint32_t a = ld_ro(M.rp + start), b = ld_ro(M.rp + start + 1);
+        __stcg(reinterpret_cast<uint4*>(M.rec), make_uint4(start, a, b - a, 0u));
+        if (write_perm)
+            M.perm[reverse ? M.n - 1 : 0] = start;
+        s.vis[start >> 5] |= 1u << (start & 31);
+    }
+    gsync<B>();
+    uint32_t head = 0, tail = 1, lvl_end = 1, L = 0, lstart = 0;
+    bool carry = false;  // the chunk's parents are the last chunk's children, still in shared memory
+    while (head < tail) {
+        if (head == lvl_end) {
+            L += 1;
+            lstart = head;
+            lvl_end = tail;
+        }
+        uint32_t m;
+        if (carry) {
+            so.form_from_children();
+            m = s.m;
+        } else {
+            m = so.form(head, lvl_end);
+        }
+        // a whole level in one chunk whose children fit one chunk: they are
+        // the next chunk's parents
+        const bool whole_level = head + m == lvl_end && head + m == tail;
+        const uint32_t q = so.step(tail, sorted, write_perm, reverse);
+        head += m;
+        tail += q;
+        carry = whole_level && q > 0 && q <= (uint32_t)B && s.Qdeg <= (uint32_t)EMAX;
+        if (tail > M.n) {  // cannot happen on a valid run
+            if (t == 0)
+                set_status(M.res, kErrCheck, 604);
+            break;
+        }
+    }
+    placed = tail;
+    nlevels = L + 1;
+    last_start = lstart;
+}
+
+// Full reorder of one matrix by one solo group: start search
+// (simple_peripheral.cpp:92-141), the sorted pass, reverse, bandwidth.
+// e2: the matrix's edge records; inv: n words for the inverse permutation.
+template <int B, int EMAX>
+__device__ void solo_reorder(SoloSmem<B, EMAX>& s, const MatrixView& M, const uint4* e2, uint32_t* inv,
+                             const Options& opt)
+{
+    const uint32_t t = gtid<B>();
+    const uint32_t n = M.n;
+    if (t == 0)
+        M.res->t_begin = globaltimer();
+    Solo<B, EMAX> so{s, M, e2};
+    uint32_t start = opt.start;
+    if (start != kUnvisited && start >= n) {
+        if (t == 0)
+            set_status(M.res, kErrArg, 2);
+        return;
+    }
+    uint32_t passes = 0, ecc = 0, placed = 0, nlevels = 0, last_start = 0;
+    bool searching = start == kUnvisited && n > 1;
+    if (n == 1) {
+        passes = start == kUnvisited ? 1 : 0;
+        start = 0;
+    } else if (searching) {
+        start = n / 2;
+    }
+    uint32_t lastdist = 0;
+    while (true) {
+        if (!searching && opt.mode == kModeStartOnly)
+            break;
+        if (searching)
+            ++passes;
+        solo_pass<B, EMAX>(so, start, !searching, !searching, opt.reverse != 0, placed, nlevels, last_start);
+        if (read_status(M.res) != 0)
+            return;
+        if (!searching)
+            break;
+        if (placed != n) {
+            if (t == 0)
+                set_status(M.res, kErrDisconnected, 0);
+            return;
+        }
+        const uint32_t dist = nlevels - 1;
+        if (dist == lastdist) {
+            ecc = dist;
+            searching = false;  // the sorted pass from the same start comes next
+            continue;
+        }
+        if (t == 0)
+            s.bcast[0] = next_peripheral_start(M, opt.outnodes, last_start);
+        gsync<B>();
+        start = s.bcast[0];
+        gsync<B>();
+        lastdist = dist;
+        if (passes > n) {
+            if (t == 0)
+                set_status(M.res, kErrCheck, 3);
+            return;
+        }
+    }
+    if (opt.mode == kModeStartOnly) {
+        if (t == 0) {
+            M.res->start = start;
+            M.res->passes = passes;
+            M.res->ecc = ecc;
+            M.res->placed = n;
+        }
+        return;
+    }
+    if (placed != n) {
+        if (t == 0) {
+            set_status(M.res, kErrDisconnected, 1);
+            M.res->placed = placed;
+        }
+        return;
+    }
+    if (opt.want_bw) {
+        for (uint32_t pos = t; pos < n; pos += B)
+            inv[__ldcg(&M.rec[pos].node)] = pos;
+        gsync<B>();
+        unsigned long long bw = 0, bw0 = 0, plo = 0, phi = 0;
+        for (uint32_t i = t; i < n; i += B) {
+            const uint32_t a = ld_ro(M.rp + i), e = ld_ro(M.rp + i + 1);
+            if (a == e)
+                continue;
+            const uint32_t me = __ldcg(inv + i);
+            uint32_t mnr = kUnvisited, mxr = 0;
+            for (uint32_t k = a; k < e; ++k) {
+                const uint32_t p = __ldcg(inv + ld_ro(M.ci + k));
+                mnr = min(mnr, p);
+                mxr = max(mxr, p);
+            }
+            // computeBandwidth (main.cpp:143-184): max(row - min, max - row)
+            const unsigned long long b1 = me >= mnr ? (unsigned long long)(me - mnr) : 0ull;
+            const unsigned long long b2 = mxr >= me ? (unsigned long long)(mxr - me) : 0ull;
+            bw = max(bw, max(b1, b2));
+            plo += b1;
+            phi += b2;
+            // initial bandwidth: first / last stored column (main.cpp:114-129)
+            const uint32_t c0 = ld_ro(M.ci + a), c1 = ld_ro(M.ci + e - 1);
+            const unsigned long long i0 = i >= c0 ? i - c0 : 0, i1 = c1 >= i ? c1 - i : 0;
+            bw0 = max(bw0, max(i0, i1));
+        }
+        bw = block_reduce_max<B, unsigned long long>(bw, s.tmp64);
+        bw0 = block_reduce_max<B, unsigned long long>(bw0, s.tmp64);
+        block_reduce_sum2<B>(plo, phi, s.tmp64);
+        if (t == 0) {
+            M.res->bandwidth = bw;
+            M.res->initial_bw = bw0;
+            M.res->profile_lo = plo;
+            M.res->profile_hi = phi;
+        }
+    }
+    if (t == 0) {
+        M.res->start = start;
+        M.res->passes = passes;
+        M.res->ecc = ecc;
+        M.res->levels = nlevels;
+        M.res->placed = placed;
+        M.res->t_end = globaltimer();
+    }
+}
+
+}  // namespace pbrcm

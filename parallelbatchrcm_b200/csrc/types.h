@@ -71,6 +71,8 @@ struct alignas(16) DevResult {
     unsigned long long initial_bw;
     unsigned long long profile_lo;     // sum inv[i] - min(inv[row])   (CM order)
     unsigned long long profile_hi;     // sum max(inv[row]) - inv[i]   (reversed order)
+    unsigned long long t_begin;        // %globaltimer (ns) when the engine took the matrix
+    unsigned long long t_end;          // %globaltimer (ns) when its result was written
 };
 
 // One matrix as the engine sees it.
@@ -91,6 +93,10 @@ struct MatrixView {
 };
 
 constexpr uint64_t kMaxNnz = 0xFFFFFFF0ull;
+
+// The one-group engine of the batch kernels (solo.cuh) keeps a matrix's
+// visited set in shared memory: matrices of at most this many nodes.
+constexpr uint32_t kSoloMaxN = 1u << 18;
 
 // Bytes of the per-launch team words of a cooperative launch of `ctas` CTAs:
 // 2 x u64 per CTA for the level all-gather, then one u32 barrier flag per
@@ -118,6 +124,10 @@ struct BatchJob {
     uint32_t pad;
     GridSync* gs;                 // team > 1: zeroed GridSync of this job
     unsigned long long* words;    // team > 1: zeroed team_words_bytes(team)
+    const uint32_t* ready;        // nonzero once the matrix's CSR is in device memory (written by a
+                                  // host-to-device copy after the CSR's copies); nullptr: already there
+    uint4* e2;                    // nnz edge records for the one-group engine (solo.cuh), or nullptr
+    uint32_t* inv;                // n words (the solo engine's inverse permutation)
 };
 
 // One entry of the batch work list: member `rank` of job `job`'s team.
@@ -139,6 +149,7 @@ struct Options {
     uint32_t spec_from;     // speculative split from this search pass on (0: only for solo-dominated matrices)
     uint32_t wide_at;       // first BFS pass (key base 2 nnz + 3): a level of at least this many nodes
                             // hands the matrix to the level-synchronous engine (kNeedWide; 0 = never)
+    unsigned long long data_wait_ns;  // batch kernels: bound of the wait for a matrix's CSR to arrive
 };
 
 // State of the level-synchronous engine (wide.cu), one per matrix in device

@@ -27,14 +27,15 @@ from typing import Iterable, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import AUTO_START, DEBUG_PHANTOM_CTA, Matrix, Options, Result, SessionConfig, SessionStats
+from ._lib import AUTO_START, DEBUG_PHANTOM_CTA, Matrix, Options, Result, SessionConfig, SessionStats, Tuning
 
 __all__ = [
     "PbrcmError", "Context", "default_options", "reorder", "reorder_device", "reorder_device_noalloc",
     "find_peripheral",
     "bandwidth", "reorder_batch", "reorder_batch_device", "Session", "load_mtx", "prepare_csr", "connect_device",
     "permute",
-    "permute_device", "store_mtx", "load_hicsr", "store_hicsr",
+    "permute_device", "store_mtx", "load_hicsr", "store_hicsr", "autotune", "tuning_get", "tuning_set",
+    "tuning_load",
     "Graph", "GPU_BATCH", "SimplePeripheral", "compute_bandwidth", "check_bandwidth", "max_valency",
     "check_permutation", "AUTO_START", "DEBUG_PHANTOM_CTA",
 ]
@@ -195,16 +196,24 @@ def bandwidth(row_ptr, col_idx, perm, ctx: Context | None = None):
 
 
 def reorder_batch(mats: Sequence, *, reverse: bool = True, start: int | None = None, want_bandwidth: bool = True,
-                  ctx: Context | None = None, raise_on_error: bool = True, **opt_kw):
+                  ctx: Context | None = None, raise_on_error: bool = True, perms_out: Sequence | None = None,
+                  **opt_kw):
     """Reorders many (row_ptr, col_idx) host matrices in one persistent
-    launch.  Returns (list of perms, list of result dicts)."""
+    launch.  perms_out: optional uint32 host arrays (n entries each, e.g.
+    pinned) that receive the permutations.  Returns (list of perms, list of
+    result dicts)."""
     keep = []
     arr = (Matrix * len(mats))()
     perms = []
     for i, m in enumerate(mats):
         rp, ci = _u32(m[0]), _u32(m[1])
         n = rp.shape[0] - 1
-        p = np.empty(max(n, 1), dtype=np.uint32)
+        if perms_out is not None:
+            p = perms_out[i]
+            if p.dtype != np.uint32 or not p.flags.c_contiguous or p.shape[0] < n:
+                raise ValueError("perms_out[i] must be a contiguous uint32 array of n entries")
+        else:
+            p = np.empty(max(n, 1), dtype=np.uint32)
         keep += [rp, ci]
         perms.append(p)
         arr[i].row_ptr = rp.ctypes.data
@@ -241,6 +250,48 @@ def reorder_batch_device(mats: Sequence, *, reverse: bool = True, ctx: Context |
     if raise_on_error:
         _check(rc, "pbrcm_reorder_batch_device")
     return [r.as_dict() for r in res]
+
+
+def autotune(mats: Sequence, *, ctx: Context, cache_path: str | None = None, reverse: bool = True,
+             **opt_kw) -> dict:
+    """Measures the batch and serving shapes on a calibration batch of
+    (row_ptr, col_idx) host matrices (pbrcm_autotune): the chosen settings
+    become ctx's and, with cache_path, are written there.  Returns them."""
+    keep = []
+    arr = (Matrix * len(mats))()
+    for i, m in enumerate(mats):
+        rp, ci = _u32(m[0]), _u32(m[1])
+        keep += [rp, ci]
+        arr[i].row_ptr = rp.ctypes.data
+        arr[i].col_idx = ci.ctypes.data
+        arr[i].n = rp.shape[0] - 1
+        arr[i].nnz = ci.shape[0]
+        arr[i].perm_out = None
+    o = default_options(reverse=reverse, **opt_kw)
+    t = Tuning()
+    path = cache_path.encode() if cache_path else None
+    _check(_lib.lib().pbrcm_autotune(ctx.handle, arr, len(mats), ctypes.byref(o), path, ctypes.byref(t)),
+           "pbrcm_autotune")
+    return t.as_dict()
+
+
+def tuning_get(ctx: Context) -> dict:
+    t = Tuning()
+    _check(_lib.lib().pbrcm_tuning_get(ctx.handle, ctypes.byref(t)), "pbrcm_tuning_get")
+    return t.as_dict()
+
+
+def tuning_set(ctx: Context, **kw) -> None:
+    """Sets some of the context's batch / serving settings (the others stay)."""
+    t = Tuning()
+    _check(_lib.lib().pbrcm_tuning_get(ctx.handle, ctypes.byref(t)), "pbrcm_tuning_get")
+    for k, v in kw.items():
+        setattr(t, k, v)
+    _check(_lib.lib().pbrcm_tuning_set(ctx.handle, ctypes.byref(t)), "pbrcm_tuning_set")
+
+
+def tuning_load(ctx: Context, path: str) -> None:
+    _check(_lib.lib().pbrcm_tuning_load(ctx.handle, path.encode()), "pbrcm_tuning_load")
 
 
 class Session:

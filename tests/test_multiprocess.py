@@ -58,7 +58,8 @@ def test_reference_arm_under_torchrun_two_ranks():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes", "1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
            os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0"]
-    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
+    env = dict(os.environ, PBRCM_BENCH_COUNT="48")  # a short stream: this checks the plumbing
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
     assert r.returncode == 0, r.stderr[-3000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1, r.stdout
@@ -68,7 +69,8 @@ def test_reference_arm_under_torchrun_two_ranks():
 
 def test_batch_shards_by_nnz():
     sys.path.insert(0, ROOT)
-    from parallelbatchrcm_b200 import gen, workloads
+    import bench_workloads as workloads
+    from parallelbatchrcm_b200 import gen
     specs = gen.mixed_batch_specs(count=300, seed=42)
     est = [gen.spec_nnz_estimate(s) for s in specs]
     shards = workloads.shard_by_nnz(est, 3)
