@@ -23,7 +23,9 @@ workload (rank 0; other ranks exit 0).  Under torchrun every rank reorders
 its own 4,096 matrices (weak scaling; no exchange between GPUs); value is the
 sum over ranks of reorders / the max over ranks of the timed time.
 
---workload single|batch|serve|permute|connect|wide run one part alone
+--workload single|batch|serve|permute|connect|wide run one part alone;
+refgpu times the reference's own GPU_SIMPLE beside this engine, cpu the
+reference's serial and CPU_BATCH paths on the single-matrix configurations
 (bench_workloads.py).
 """
 from __future__ import annotations
@@ -45,8 +47,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed",
-                    choices=["mixed", "single", "batch", "serve", "permute", "connect", "wide"])
+                    choices=["mixed", "single", "batch", "serve", "permute", "connect", "wide", "refgpu", "cpu"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lean", action="store_true",
+                    help="batched launches only (no plain pass, e2e, serving, 128^3 grid or CPU legs): for profiling")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     try:

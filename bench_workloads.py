@@ -326,10 +326,14 @@ def _plain_pass(P, ctx, dmats, stream):
 
 
 def _serve_session(P, ctx, mats, arrivals, streams=96):
+    """Submits each request at its arrival time from a thread; once all are
+    in, drains the session and reads every result.  Latency = the arrival's
+    delay to submission + the session's own submit -> completion time, so
+    that no polling loop competes with the session's worker."""
     sess = P.Session(ctx, streams=streams)
     n = len(mats)
     tick = [None] * n
-    done_at = [None] * n
+    t_sub = [0.0] * n
     t0 = time.perf_counter() + 0.05
 
     def submitter():
@@ -339,26 +343,20 @@ def _serve_session(P, ctx, mats, arrivals, streams=96):
                 if d <= 0:
                     break
                 time.sleep(min(d, 0.001))
+            t_sub[i] = time.perf_counter()
             tick[i] = sess.submit(mats[i][0], mats[i][1])
 
     th = threading.Thread(target=submitter)
     th.start()
-    pending = set(range(n))
-    perms = [None] * n
-    while pending:
-        for i in list(pending):
-            if tick[i] is None:
-                continue
-            out = sess.poll(tick[i])
-            if out is not None:
-                done_at[i] = time.perf_counter()
-                assert out[1]["status"] == 0, out[1]
-                perms[i] = out[0]
-                pending.discard(i)
-        time.sleep(0.0002)
     th.join()
-    lat = [(done_at[i] - (t0 + arrivals[i])) * 1e3 for i in range(n)]
-    makespan = max(done_at) - t0
+    sess.drain()
+    lat, perms = [], []
+    for i in range(n):
+        out = sess.poll(tick[i])
+        assert out is not None and out[1]["status"] == 0, out
+        perms.append(out[0])
+        lat.append((t_sub[i] - (t0 + arrivals[i])) * 1e3 + out[1]["total_ms"])
+    makespan = max(arrivals[i] + lat[i] / 1e3 for i in range(n))
     sess.close()
     return lat, makespan, perms
 
@@ -380,7 +378,10 @@ def _serve_plain(P, ctx, mats, arrivals):
 
 def measure_serve(P, ctx, mats, gaps, rates):
     """Session (continuous batching) against the plain FIFO worker at each
-    arrival rate; both from host buffers, latency = arrival -> result."""
+    arrival rate; both from host buffers, latency = arrival -> result.  One
+    untimed pass of the session first: it fills the context's pinned
+    staging pool, as a running service would have it."""
+    _serve_session(P, ctx, mats, [0.0] * len(mats))
     rows = []
     for rate in rates:
         arr = list(np.asarray(gaps) / rate)
@@ -471,6 +472,9 @@ def run_mixed(args, ws, rank, local, extras: bool = True):
     import torch
 
     import parallelbatchrcm_b200 as P
+
+    if getattr(args, "lean", False):
+        return run_batch_lean(args, ws, rank, local)
 
     count = int(os.environ.get("PBRCM_BENCH_COUNT", "4096"))
     serve_n = int(os.environ.get("PBRCM_BENCH_SERVE", "160")) if ws == 1 and extras else 0
@@ -606,6 +610,35 @@ def run_mixed(args, ws, rank, local, extras: bool = True):
         "gpu_launches": 2 * args.steps,
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch_lean(args, ws, rank, local):
+    """Only the batched launches of the default workload (PBRCM_BENCH_COUNT
+    matrices): W + K steps of pbrcm_reorder_batch_device, one JSON line with
+    their event time.  Made for profiling, where every other leg would add
+    thousands of launches."""
+    import torch
+
+    import parallelbatchrcm_b200 as P
+
+    count = int(os.environ.get("PBRCM_BENCH_COUNT", "4096"))
+    mats = generate(mixed_specs(count, ws, rank))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ctx = P.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    dmats = _upload(mats, dev)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        _batched_step(P, ctx, dmats, stream)
+    times = [_batched_step(P, ctx, dmats, stream)[0] for _ in range(args.steps)]
+    if rank == 0:
+        sum_nnz = sum(int(ci.shape[0]) for _, ci in mats)
+        print(json.dumps({"metric": METRIC, "value": count * len(times) / (sum(times) / 1e3), "unit": "reorders/s",
+                          "ms_per_step": statistics.mean(times), "config": {"workload": f"mixed_batch_{count}",
+                                                                            "sum_nnz": sum_nnz, "lean": True}}),
+              flush=True)
     return 0
 
 
@@ -963,13 +996,109 @@ def run_wide(args, ws, rank, local):
     return 0
 
 
+def _single_configs():
+    """The single-matrix configurations: 64^2 and 128^3 grids, 1M-point RGG."""
+    return [("grid2d_64x64", lambda: gen.grid2d(64, 64, seed=1)),
+            ("grid3d_128^3", lambda: gen.grid3d(128, 128, 128, seed=12345)),
+            ("rgg_1M_k6-14", lambda: gen.rgg(1_000_000, seed=7))]
+
+
+def run_refgpu(args, ws, rank, local):
+    """The reference's own GPU path GPU_SIMPLE (src/device/rcm_gpu.cu,
+    compiled unchanged for sm_100a: oracle/_ref/ref_gpu_simple) beside this
+    engine on the single-matrix configurations, both from the start node the
+    reference's findPeripheral picks (the time of one Cuthill-McKee pass, as
+    GPU_SIMPLE::rcm reports it: mean of 20 runs after 5 warm-ups).  Also
+    counts where GPU_SIMPLE's order differs from the serial stable one.  The
+    reference's GPU_BATCH kernel is not run: its waits are unbounded and it
+    traps on an internal overflow (include/device/batchWorker.cuh:213-279,
+    539-543)."""
+    import torch
+
+    import parallelbatchrcm_b200 as P
+    if rank != 0:
+        return 0
+    O = _oracle()
+    torch.cuda.set_device(local)
+    ctx = P.Context(local)
+    dev = torch.device("cuda", local)
+    rows = []
+    for name, make in _single_configs():
+        m = make()
+        start, _, _ = O.peripheral(m.row_ptr, m.col_idx)
+        cm = O.cm_order(m.row_ptr, m.col_idx, start)
+        ref = O.ref_gpu_simple(m.row_ptr, m.col_idx, start)
+        rp = torch.from_numpy(m.row_ptr.view(np.int32)).to(dev)
+        ci = torch.from_numpy(m.col_idx.view(np.int32)).to(dev)
+        po = torch.empty(m.n, dtype=torch.int32, device=dev)
+        ms = []
+        for i in range(25):
+            _, r = P.reorder_device(rp, ci, po, reverse=False, start=int(start), want_bandwidth=False, ctx=ctx)
+            if i >= 5:
+                ms.append(r["device_ms"])
+        ours = po.cpu().numpy().view(np.uint32)
+        row = {"workload": name, "n": m.n, "nnz": m.nnz, "start": int(start),
+               "ours_ms": statistics.mean(ms), "ours_equals_serial_stable": bool(np.array_equal(ours, cm)),
+               "ours_bandwidth": O.bandwidth(m.row_ptr, m.col_idx, ours)}
+        if ref is not None:
+            rms, rperm = ref
+            row.update({"gpu_simple_ms": rms, "gpu_simple_positions_differing": int((rperm != cm).sum()),
+                        "gpu_simple_bandwidth": O.bandwidth(m.row_ptr, m.col_idx, rperm),
+                        "speedup": rms / statistics.mean(ms)})
+        rows.append(row)
+        log(json.dumps(row))
+    print(json.dumps({"metric": "ms per Cuthill-McKee pass from a given start (reference GPU_SIMPLE vs ours)",
+                      "rows": rows, "gpu_batch": "not run: unbounded device waits and a reachable __trap "
+                                                 "(include/device/batchWorker.cuh:213-279, 539-543)"}), flush=True)
+    return 0
+
+
+def run_cpu(args, ws, rank, local):
+    """The reference's CPU paths on the single-matrix configurations, on this
+    host: findPeripheral + RealCPU::rcm<true> serial (rcm_seq) and CPU_BATCH
+    with 2..nproc threads (batch 512), as src/main.cpp:456-483 runs them; each
+    RealCPU::rcm reports the mean of its 25 internal repetitions."""
+    if rank != 0:
+        return 0
+    import platform
+    nproc = os.cpu_count() or 1
+    threads = [t for t in (1, 2, 4, 8, 16, 32, 64) if t <= nproc]
+    if threads[-1] != nproc:
+        threads.append(nproc)
+    rows = []
+    for name, make in _single_configs():
+        m = make()
+        row = {"workload": name, "n": m.n, "nnz": m.nnz}
+        for t in threads:
+            ms, kind, _ = reference_single(m.row_ptr, m.col_idx, 1, t)
+            row[f"threads_{t}_reorder_ms"] = ms[0]
+        O = _oracle()
+        rr = O.ref_time(m.row_ptr, m.col_idx, 1, 1)[0]
+        row["peripheral_ms"] = rr["peripheral_ms"]
+        row["serial_rcm_ms"] = rr["rcm_ms"]
+        rows.append(row)
+        log(json.dumps(row))
+    cpu_model = platform.processor() or ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    cpu_model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    print(json.dumps({"metric": "ms per full reorder on the host (reference CPU code)", "cpu": cpu_model,
+                      "nproc": nproc, "rows": rows}), flush=True)
+    return 0
+
+
 def main(args, ws, rank, local):
     if args.impl == "reference":
         if args.workload == "single":
             return run_single_reference(args, ws, rank)
         return run_mixed_reference(args, ws, rank)
     fn = {"mixed": run_mixed, "single": run_single, "serve": run_serve, "permute": run_permute,
-          "connect": run_connect, "wide": run_wide}.get(args.workload)
+          "connect": run_connect, "wide": run_wide, "refgpu": run_refgpu, "cpu": run_cpu}.get(args.workload)
     if args.workload == "batch":
         return run_mixed(args, ws, rank, local, extras=False)
     if fn is None:

@@ -215,14 +215,16 @@ PBRCM_API int32_t pbrcm_reorder_batch_device(pbrcm_context* ctx, const pbrcm_mat
  * one batch shape for every input; here they are measured per device.
  */
 typedef struct pbrcm_tuning {
-    uint32_t batch_pool;       /* thread groups per 512-thread CTA of the batch kernel:
-                                  0 = 1 x 512 threads, 1 = 2 x 256, 2 = 4 x 128, 3 = 8 x 64 */
+    uint32_t batch_pool;       /* thread groups of the batch kernel, one matrix each:
+                                  0 = 1 x 512 threads per CTA, 1 = 2 x 256, 2 = 4 x 128,
+                                  3 = 8 x 64, 5 = 256-thread CTAs with 512-edge chunks, three
+                                  per SM */
     uint32_t cluster_size;     /* CTAs of a cluster team for the biggest matrices (1 = none) */
     uint32_t cluster_max;      /* at most this many matrices of a batch get a cluster team */
     uint32_t cluster_nnz;      /* ... and only those with at least this many entries */
     uint32_t session_cutoff_n; /* serving: requests with more nodes run on a cooperative team */
     uint32_t session_pool;     /* serving: CTA shape of the other requests (0 = 512 threads,
-                                  4 = 128 threads, four per SM) */
+                                  5 = 256 threads, three per SM, 4 = 128 threads, four per SM) */
     uint32_t sms;              /* streaming multiprocessors of the device it was measured on */
     uint32_t trials;           /* settings measured */
     uint32_t source;           /* 0 built-in defaults, 1 a tuning file, 2 measured or set */

@@ -19,6 +19,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpbrcm_oracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "ref_rcm")
+REF_GPU_BIN = os.path.join(HERE, "_ref", "ref_gpu_simple")
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _lib = None
@@ -237,6 +238,23 @@ def ref_time(rp, ci, threads: int, steps: int, timeout: float | None = None):
                             str(threads), str(steps)], capture_output=True, text=True, check=True,
                            timeout=timeout)
     return [json.loads(line[5:]) for line in r.stdout.splitlines() if line.startswith("JSON ")]
+
+
+def ref_gpu_simple(rp, ci, start: int, timeout: float | None = 600):
+    """The reference's own GPU_SIMPLE::rcm (src/device/rcm_gpu.cu) from
+    `start` (oracle/_ref/ref_gpu_simple): (mean ms of its 20 timed runs, CM
+    order).  None if that build is missing."""
+    if not os.path.exists(REF_GPU_BIN):
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        _u32(rp).tofile(os.path.join(td, "rp"))
+        _u32(ci).tofile(os.path.join(td, "ci"))
+        out = os.path.join(td, "out")
+        r = subprocess.run([REF_GPU_BIN, os.path.join(td, "rp"), os.path.join(td, "ci"), str(int(start)), out],
+                           capture_output=True, text=True, check=True, timeout=timeout)
+        info = _parse_json(r.stdout)
+        perm = np.fromfile(out + ".perm", dtype=np.uint32)
+    return info["ms"], perm
 
 
 def write_pack(path: str, mats) -> None:

@@ -156,14 +156,18 @@ int32_t Context::init(int dev)
     wide_batch_pass = env_int("PBRCM_WIDE_BATCH_PASS", 1) != 0;
     wide_ctas = wide_ctas_per_sm() * sms;
     // batch / serving shape: built-in defaults (measured on the 4,096-matrix
-    // mixed batch: 212 / 178 / 220 / 382 ms for 1 x 512, 2 x 256, 4 x 128,
-    // 8 x 64 threads per group), or a tuning file written by pbrcm_autotune
+    // mixed batch with the solo engine: 132 / 106 / 153 ms for 1 x 512,
+    // 2 x 256, 4 x 128 threads per group; without it 212 / 178 / 220 / 382
+    // ms for 1 x 512 .. 8 x 64), or a tuning file written by pbrcm_autotune
     // for this device shape and library version (PBRCM_TUNING); a PBRCM_*
     // knob below still overrides a single setting
     pbrcm_tuning tn;
     std::memset(&tn, 0, sizeof(tn));
     tn.batch_pool = 1;
-    tn.cluster_size = 2;
+    // no cluster teams by default: with the solo engine one group takes even
+    // the biggest matrices of the mixed batch faster than a cluster team of
+    // the engine does (100 ms against 106 ms for the 4,096-matrix batch)
+    tn.cluster_size = 1;
     tn.cluster_max = 16;
     tn.cluster_nnz = 1u << 18;
     tn.session_cutoff_n = 1u << 18;
@@ -173,11 +177,14 @@ int32_t Context::init(int dev)
             tuned = 1;
     }
     batch_pool = env_int("PBRCM_BATCH_POOL", (int)tn.batch_pool);
-    if (batch_pool < 0 || batch_pool > 3)
+    if (batch_pool < 0 || batch_pool > 5 || batch_pool == 4)
         batch_pool = 1;
     session_cutoff_n = (uint32_t)std::max(1, env_int("PBRCM_SESSION_CUTOFF_N", (int)tn.session_cutoff_n));
-    session_pool = env_int("PBRCM_SESSION_POOL", (int)tn.session_pool) == 4 ? 4 : 0;
-    solo = env_int("PBRCM_SOLO", 0) != 0;
+    session_pool = env_int("PBRCM_SESSION_POOL", (int)tn.session_pool);
+    if (session_pool != 0 && session_pool != 4 && session_pool != 5)
+        session_pool = 0;
+    solo = env_int("PBRCM_SOLO", 1) != 0;
+    batch_graphs = env_int("PBRCM_BATCH_GRAPHS", 1) != 0;
     if (cudaMalloc(&d_agg, kTeamParts * team_part_bytes(maxc)) != cudaSuccess)
         return PBRCM_ERR_OOM;
     // cluster teams of the batch path (PBRCM_BATCH_CLUSTER* override)
@@ -203,6 +210,11 @@ Context::~Context()
                     (void*)d_arena})
         if (p)
             cudaFree(p);
+    if (bgraph.exec)
+        cudaGraphExecDestroy(bgraph.exec);
+    for (void* p : {(void*)h_jobs, (void*)h_slots, (void*)h_bres})
+        if (p)
+            cudaFreeHost(p);
     if (d_ready)
         cudaFree(d_ready);
     if (h_one)

@@ -3,7 +3,9 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <mutex>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -35,13 +37,14 @@ struct Context {
     bool wide_batch_pass = true;   // batches sized by the last pass's levels (else 8, 16, 32, ...)
     int wide_ctas = 0;  // CTAs per level step (0: engine unavailable)
     // batches: the biggest matrices go to thread-block-cluster teams
-    int cluster_size = 2;             // CTAs per cluster (0 or 1: off)
+    int cluster_size = 1;             // CTAs per cluster (0 or 1: off)
     uint64_t cluster_nnz = 1u << 18;  // matrices with at least this many entries
     int cluster_max = 16;             // cap on the matrices given a cluster (0: one per co-resident cluster)
     uint32_t cluster_solo_parents = 0, cluster_solo_edges = 0;  // solo level bounds inside a cluster
     // serving: a request of more nodes runs on a cooperative team
     uint32_t session_cutoff_n = 1u << 18;
-    int session_pool = 0;  // serving: kPools shape of the one-CTA requests
+    int session_pool = 0;  // serving: kPools shape of the one-CTA requests (512-thread CTAs: on the
+                           // Poisson mix 264 reorders/s against 219 for 256-thread CTAs)
     // where the batch / serving shape came from: 0 built-in defaults, 1 a
     // tuning file, 2 pbrcm_autotune or pbrcm_tuning_set
     uint32_t tuned = 0;
@@ -93,6 +96,28 @@ struct Context {
     uint32_t* d_ready = nullptr;
     size_t cap_ready = 0;
     uint32_t* h_one = nullptr;
+    // pinned staging of a batch's job list and results (grow only)
+    BatchJob* h_jobs = nullptr;
+    size_t cap_hjobs = 0;
+    BatchSlot* h_slots = nullptr;
+    size_t cap_hslots = 0;
+    DevResult* h_bres = nullptr;
+    size_t cap_hbres = 0;
+    // host-buffer batches over pinned memory are captured as one CUDA graph
+    // (copies in, kernel, results and permutations out) and replayed while
+    // the same buffers, options and shape come back (PBRCM_BATCH_GRAPHS=0:
+    // never)
+    bool batch_graphs = true;
+    // serving sessions' pinned staging pool, shared by the context's sessions
+    // (created by the first session; type private to session.cpp)
+    std::shared_ptr<void> session_pinned;
+    struct BatchGraph {
+        uint64_t key = 0;
+        cudaGraphExec_t exec = nullptr;
+        std::vector<uint32_t> order;  // job q -> matrix index
+        std::vector<BatchJob> jobs;
+        uint64_t replays = 0;
+    } bgraph;
 
     int32_t init(int dev);
     ~Context();

@@ -1861,6 +1861,7 @@ __device__ void validate_group(const MatrixView& M, uint32_t* red)
     }
     if (t == 0 && (ld_ro(M.rp) != 0 || ld_ro(M.rp + M.n) != M.nnz))
         bad = true;
+#pragma unroll 4
     for (uint32_t k = t; k < M.nnz; k += B)
         if (ld_ro(M.ci + k) >= M.n)
             bad = true;

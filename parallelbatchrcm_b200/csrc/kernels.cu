@@ -189,6 +189,7 @@ const PoolInfo kPools[kNumPools] = {
     {512, 2048, 128, 512},
     {512, 2048, 64, 256},
     {128, 512, 128, 512},
+    {256, 512, 256, 512},
 };
 
 #define PBRCM_DISPATCH(v, CALL)                     \
@@ -200,8 +201,9 @@ const PoolInfo kPools[kNumPools] = {
     }
 
 // the pool shapes' entry points (pool_p<N>.cu, one translation unit each)
-extern const PoolFns kPoolFns0, kPoolFns1, kPoolFns2, kPoolFns3, kPoolFns4;
-static const PoolFns* const kPoolTable[kNumPools] = {&kPoolFns0, &kPoolFns1, &kPoolFns2, &kPoolFns3, &kPoolFns4};
+extern const PoolFns kPoolFns0, kPoolFns1, kPoolFns2, kPoolFns3, kPoolFns4, kPoolFns5;
+static const PoolFns* const kPoolTable[kNumPools] = {&kPoolFns0, &kPoolFns1, &kPoolFns2,
+                                                     &kPoolFns3, &kPoolFns4, &kPoolFns5};
 
 size_t variant_smem(int v)
 {

@@ -1,9 +1,10 @@
 // pool.cuh -- the batch kernels: many matrices in one launch, several thread
 // groups per CTA, the biggest matrices on thread-block-cluster teams.
 //
-// A "pool" shape is <B, EMAX, GB, GE>: CTAs of B threads (a cluster team of
-// whole CTAs chunks EMAX edges per CTA) split into B / GB thread groups of GB
-// threads that reorder one matrix each (GE edges per chunk).  Each shape is
+// A "pool" shape is <B, EMAX, GB, GE, MINB>: CTAs of B threads (a cluster
+// team of whole CTAs chunks EMAX edges per CTA) split into B / GB thread
+// groups of GB threads that reorder one matrix each (GE edges per chunk),
+// compiled for MINB CTAs per SM.  Each shape is
 // instantiated in its own translation unit (pool_p<N>.cu) through
 // PBRCM_DEFINE_POOL, which exports its entry points as a PoolFns table.
 #pragma once
@@ -87,11 +88,13 @@ __device__ void group_take_slots(unsigned char* raw, const BatchJob* jobs, const
         if (!prepare_job<GB>(s, job, opt))
             continue;
         if constexpr (solo_fits<B, GB, GE>()) {
-            // one group alone on a matrix whose visited set fits shared
-            // memory and whose rows fit a chunk: the solo engine
-            if (job.e2 != nullptr && job.team == 1 && job.M.n <= kSoloMaxN && read_status(job.M.res) == 0 &&
-                __ldcg(&job.M.res->maxdeg) <= (uint32_t)GE) {
-                solo_reorder<GB, GE>(*reinterpret_cast<SoloSmem<GB, GE>*>(raw), job.M, job.e2, job.inv, opt);
+            // one group alone on a matrix whose rows fit a chunk: the solo
+            // engine (visited bitmap in shared memory, or in global memory
+            // for a matrix over kSoloMaxN nodes)
+            if (job.e2 != nullptr && job.team == 1 && (job.M.n <= kSoloMaxN || job.gvis != nullptr) &&
+                read_status(job.M.res) == 0 && __ldcg(&job.M.res->maxdeg) <= (uint32_t)GE) {
+                solo_reorder<GB, GE>(*reinterpret_cast<SoloSmem<GB, GE>*>(raw), job.M, job.e2, job.inv,
+                                     job.M.n > kSoloMaxN ? job.gvis : nullptr, opt);
                 gsync<GB>();
                 continue;
             }
@@ -119,9 +122,9 @@ __device__ void group_take_slots(unsigned char* raw, const BatchJob* jobs, const
 // thread groups, each taking slots of the work list (group_take_slots), so
 // that several matrices are in flight per SM.  The launch is cooperative
 // when some job has a team of several groups (every member resident).
-template <int B, int GB, int GE>
-__global__ void __launch_bounds__(B, 512 / B) k_reorder_batch(const BatchJob* jobs, const BatchSlot* slots,
-                                                              uint32_t nslots, uint32_t* counter, Options opt)
+template <int B, int GB, int GE, int MINB>
+__global__ void __launch_bounds__(B, MINB) k_reorder_batch(const BatchJob* jobs, const BatchSlot* slots,
+                                                           uint32_t nslots, uint32_t* counter, Options opt)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     group_take_slots<B, GB, GE>(group_smem<B, GB, GE>(smem_raw), jobs, slots, nslots, counter, opt);
@@ -138,8 +141,8 @@ __global__ void __launch_bounds__(B, 512 / B) k_reorder_batch(const BatchJob* jo
 // remaining one-group slots from counters[1] on their own, as
 // k_reorder_batch does (no cluster barrier and no shared-memory access
 // across CTAs from then on).
-template <int B, int EMAX, int GB, int GE>
-__global__ void __launch_bounds__(B, 512 / B) k_reorder_cluster(const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots,
+template <int B, int EMAX, int GB, int GE, int MINB>
+__global__ void __launch_bounds__(B, MINB) k_reorder_cluster(const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots,
                                                           uint32_t nslots, uint32_t* counters, Options copt,
                                                           Options opt)
 {
@@ -200,8 +203,9 @@ namespace {
 
 // The batch kernels of one pool shape: CTAs of B threads (cluster teams of
 // whole CTAs, EMAX edges per chunk), split into groups of GB threads (GE
-// edges per chunk) for the one-group slots.
-template <int B, int EMAX, int GB, int GE>
+// edges per chunk) for the one-group slots; MINB CTAs per SM (the register
+// bound the kernels are compiled for).
+template <int B, int EMAX, int GB, int GE, int MINB>
 struct Pool {
     static_assert(B % GB == 0 && B / GB <= 15, "at most 15 groups (named barriers 1..15) per CTA");
     static size_t batch_smem() { return (size_t)(B / GB) * group_stride<B, GB, GE>(); }
@@ -209,15 +213,15 @@ struct Pool {
     static cudaError_t prepare()
     {
         static cudaError_t once = [] {
-            cudaError_t e = cudaFuncSetAttribute(k_reorder_batch<B, GB, GE>,
+            cudaError_t e = cudaFuncSetAttribute(k_reorder_batch<B, GB, GE, MINB>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem());
             if (e != cudaSuccess)
                 return e;
-            e = cudaFuncSetAttribute(k_reorder_cluster<B, EMAX, GB, GE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            e = cudaFuncSetAttribute(k_reorder_cluster<B, EMAX, GB, GE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)cluster_smem());
             if (e != cudaSuccess)
                 return e;
-            return cudaFuncSetAttribute(k_reorder_cluster<B, EMAX, GB, GE>,
+            return cudaFuncSetAttribute(k_reorder_cluster<B, EMAX, GB, GE, MINB>,
                                         cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         }();
         return once;
@@ -244,7 +248,7 @@ struct Pool {
         cudaLaunchAttribute at[1];
         cudaLaunchConfig_t cfg = cluster_config(csize, 1, nullptr, at);
         int n = 0;
-        if (cudaOccupancyMaxActiveClusters(&n, (void*)k_reorder_cluster<B, EMAX, GB, GE>, &cfg) != cudaSuccess) {
+        if (cudaOccupancyMaxActiveClusters(&n, (void*)k_reorder_cluster<B, EMAX, GB, GE, MINB>, &cfg) != cudaSuccess) {
             cudaGetLastError();
             return 0;
         }
@@ -259,7 +263,7 @@ struct Pool {
             return e;
         cudaLaunchAttribute at[1];
         cudaLaunchConfig_t cfg = cluster_config(csize, nclusters, st, at);
-        return cudaLaunchKernelEx(&cfg, k_reorder_cluster<B, EMAX, GB, GE>, jobs, nbig, slots, nslots, counters, copt,
+        return cudaLaunchKernelEx(&cfg, k_reorder_cluster<B, EMAX, GB, GE, MINB>, jobs, nbig, slots, nslots, counters, copt,
                                   opt);
     }
     static int batch_max_ctas(int sms)
@@ -267,7 +271,7 @@ struct Pool {
         if (prepare() != cudaSuccess)
             return 0;
         int nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_reorder_batch<B, GB, GE>, B, batch_smem()) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_reorder_batch<B, GB, GE, MINB>, B, batch_smem()) !=
             cudaSuccess)
             return 0;
         return nb * sms;
@@ -280,7 +284,7 @@ struct Pool {
             return e;
         if (!cooperative) {
             // no team: groups never wait for each other, a plain launch will do
-            k_reorder_batch<B, GB, GE><<<ctas, B, batch_smem(), st>>>(jobs, slots, nslots, counter, opt);
+            k_reorder_batch<B, GB, GE, MINB><<<ctas, B, batch_smem(), st>>>(jobs, slots, nslots, counter, opt);
             return cudaGetLastError();
         }
         const BatchJob* j = jobs;
@@ -289,7 +293,7 @@ struct Pool {
         uint32_t* c = counter;
         Options o = opt;
         void* args[] = {&j, &sl, &ns, &c, &o};
-        return cudaLaunchCooperativeKernel((const void*)k_reorder_batch<B, GB, GE>, dim3(ctas), dim3(B), args,
+        return cudaLaunchCooperativeKernel((const void*)k_reorder_batch<B, GB, GE, MINB>, dim3(ctas), dim3(B), args,
                                            batch_smem(), st);
     }
 };
@@ -298,9 +302,9 @@ struct Pool {
 
 }  // namespace pbrcm
 
-#define PBRCM_DEFINE_POOL(IDX, B, EMAX, GB, GE)                                                             \
+#define PBRCM_DEFINE_POOL(IDX, B, EMAX, GB, GE, MINB)                                                       \
     namespace pbrcm {                                                                                       \
     extern const PoolFns kPoolFns##IDX = {                                                                  \
-        &Pool<B, EMAX, GB, GE>::batch_max_ctas, &Pool<B, EMAX, GB, GE>::cluster_max_active,                 \
-        &Pool<B, EMAX, GB, GE>::batch, &Pool<B, EMAX, GB, GE>::cluster};                                    \
+        &Pool<B, EMAX, GB, GE, MINB>::batch_max_ctas, &Pool<B, EMAX, GB, GE, MINB>::cluster_max_active,     \
+        &Pool<B, EMAX, GB, GE, MINB>::batch, &Pool<B, EMAX, GB, GE, MINB>::cluster};                        \
     }

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -40,7 +41,9 @@ using Clock = std::chrono::steady_clock;
 
 inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-// Pinned host memory, recycled by size class (powers of two).
+// Pinned host memory, recycled by size class (powers of two).  One pool per
+// context, shared by its sessions (a session that starts finds the staging
+// earlier ones left behind); its own lock.
 class PinnedPool {
 public:
     ~PinnedPool()
@@ -50,6 +53,7 @@ public:
     }
     void* get(size_t bytes, size_t& cap)
     {
+        std::lock_guard<std::mutex> lk(mu_);
         size_t c = 4096;
         while (c < bytes)
             c <<= 1;
@@ -68,11 +72,13 @@ public:
     }
     void put(void* p, size_t cap)
     {
+        std::lock_guard<std::mutex> lk(mu_);
         if (p)
             free_.emplace(cap, p);
     }
 
 private:
+    std::mutex mu_;
     std::multimap<size_t, void*> free_;
 };
 
@@ -87,11 +93,14 @@ struct Request {
     unsigned char* host = nullptr;
     size_t host_cap = 0;
     size_t off_rp = 0, off_ci = 0, off_view = 0, off_perm = 0, off_res = 0;
-    // device block: [rp | ci | node | rec | perm | res | gs | counter + view | agg | hub?]
+    // device block: [rp | ci | node | rec | perm | res | gs | counter + view | agg | hub? | edge records?]
     unsigned char* dev = nullptr;
     size_t d_rp = 0, d_ci = 0, d_node = 0, d_rec = 0, d_perm = 0, d_res = 0, d_gs = 0, d_cnt = 0, d_agg = 0,
-           d_hub = 0;
-    bool team = false;
+           d_hub = 0, d_e2 = 0, d_gvis = 0;
+    bool big = false;      // above the team cutoff (or a row longer than a one-CTA chunk)
+    bool solo_able = false;  // the solo engine can take it (rows fit its chunk)
+    bool team = false;     // decided at admission: a cooperative team of CTAs
+    bool solo = false;     // decided at admission: one CTA running the solo engine
     bool cluster = false;  // team as one thread-block cluster (no hub row)
     int ctas = 1;       // CTAs of its launch (team size, or 1)
     int units = 1;      // share of the GPU it holds (see pbrcm_session::units_per_sm)
@@ -99,6 +108,10 @@ struct Request {
     cudaEvent_t ev = nullptr;
     int state = 0;  // 0 queued, 1 running, 2 done
     int32_t rc = PBRCM_OK;
+    // once done: the result and permutation, moved out of the pinned staging
+    // (which goes back to the pool at once, for the next submissions)
+    DevResult res_done{};
+    std::vector<uint32_t> perm_done;
     Clock::time_point t_submit, t_done;
 };
 
@@ -110,7 +123,7 @@ struct pbrcm_session {
     uint32_t max_inflight = 0;
     std::vector<cudaStream_t> streams;
     std::vector<int> stream_busy;  // requests in flight per stream
-    int small_pool = 0;            // shape of one-CTA requests (kPools 0: one 512-thread group; 4: 128 threads)
+    int small_pool = 0;            // shape of one-CTA requests (kPools 0, 4 or 5: 512, 128 or 256 threads)
     uint32_t team_cutoff_n = 1u << 18;
     int max_ctas = 0;              // largest team (co-resident CTAs of the team kernel)
     // GPU share in units: an SM holds units_per_sm one-CTA requests, or one
@@ -125,6 +138,7 @@ struct pbrcm_session {
     // 289 reorders/s against 202-229 for clusters of <= 4-16 CTAs
     int cluster_max = 0;
     uint64_t team_nnz = 1ull << 19;
+    uint32_t light_team_n = 1u << 14;  // under light load, requests above this many nodes get a team
 
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -137,7 +151,8 @@ struct pbrcm_session {
     std::vector<double> lat_ms;
     Clock::time_point t_first{}, t_last{};
     bool have_first = false;
-    PinnedPool pinned;
+    std::shared_ptr<PinnedPool> pinned_pool = std::make_shared<PinnedPool>();  // the context's (see PinnedPool)
+    std::vector<cudaEvent_t> free_events;  // events of retired requests, for reuse
     std::atomic<bool> stop{false};
     std::thread worker;
     cudaMemPool_t pool = nullptr;
@@ -145,13 +160,17 @@ struct pbrcm_session {
     void run();
     bool launch(Request* r);
     void retire(Request* r);
+    void decide_mode(Request* r) const;
     int choose_ctas(const Request* r) const;
 };
 
 namespace {
 
-size_t device_bytes(uint32_t n, uint64_t nnz, bool hub, int team_ctas, size_t* offs)
+size_t device_bytes(uint32_t n, uint64_t nnz, bool hub, bool solo, int team_ctas, size_t* offs)
 {
+    // room for either way a request may run (decided at admission): team
+    // words and hub scratch for a team, edge records (and a global visited
+    // bitmap over kSoloMaxN nodes) for the solo engine
     size_t o = 0;
     offs[0] = o;  // rp
     o = align16(o + 4 * ((size_t)n + 1));
@@ -174,6 +193,12 @@ size_t device_bytes(uint32_t n, uint64_t nnz, bool hub, int team_ctas, size_t* o
     offs[9] = o;  // hub
     if (hub)
         o = align16(o + 16 * std::max<uint64_t>(nnz, 1));
+    offs[10] = o;  // the solo engine's edge records
+    if (solo)
+        o = align16(o + 16 * std::max<uint64_t>(nnz, 1));
+    offs[11] = o;  // its visited bitmap, when it does not fit shared memory
+    if (solo && n > kSoloMaxN)
+        o = align16(o + 4 * (((size_t)n + 31) / 32));
     return o;
 }
 
@@ -201,6 +226,11 @@ bool pbrcm_session::launch(Request* r)
     BatchJob J{};
     J.M = M;
     J.team = 1;
+    if (r->solo) {
+        J.e2 = reinterpret_cast<uint4*>(D + r->d_e2);
+        J.inv = reinterpret_cast<uint32_t*>(D + r->d_node);
+        J.gvis = r->n > kSoloMaxN ? reinterpret_cast<uint32_t*>(D + r->d_gvis) : nullptr;
+    }
     const BatchSlot one{0, 0};
     std::memcpy(r->host + r->off_view, &J, sizeof(J));
     std::memcpy(r->host + r->off_view + sizeof(J), &one, sizeof(one));
@@ -247,9 +277,16 @@ bool pbrcm_session::launch(Request* r)
 
 void pbrcm_session::retire(Request* r)
 {
-    DevResult res;
+    DevResult& res = r->res_done;
     std::memcpy(&res, r->host + r->off_res, sizeof(res));
     r->rc = map_status(res.status);
+    if (r->rc == PBRCM_OK)
+        r->perm_done.assign(reinterpret_cast<const uint32_t*>(r->host + r->off_perm),
+                            reinterpret_cast<const uint32_t*>(r->host + r->off_perm) + r->n);
+    pinned_pool->put(r->host, r->host_cap);
+    r->host = nullptr;
+    free_events.push_back(r->ev);
+    r->ev = nullptr;
     r->state = 2;
     r->t_done = Clock::now();
     bytes_in_flight -= r->dev_bytes;
@@ -258,6 +295,21 @@ void pbrcm_session::retire(Request* r)
     ++completed;
     lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
     t_last = r->t_done;
+}
+
+// How a request runs, decided when it is admitted.  A request above the
+// cutoff (or with a row longer than a one-CTA chunk) gets a cooperative team:
+// on one CTA its thousands of BFS levels would set the p99 (measured: the
+// Poisson mix served 125 reorders/s with them on single CTAs, 220-260 with
+// teams).  A mid-size request that finds the GPU lightly loaded also gets a
+// team, for latency; under load it runs on one CTA (the solo engine where it
+// applies), which spends far fewer SM-seconds per request.
+void pbrcm_session::decide_mode(Request* r) const
+{
+    const bool light = ctas_in_use * 4 < cap_ctas && queued.size() <= 2;
+    r->team = r->big || (light && r->n > light_team_n);
+    r->solo = !r->team && r->solo_able;
+    r->cluster = r->team && cluster_max >= 2 && r->maxdeg <= (uint32_t)kPools[small_pool].gemax;
 }
 
 // CTAs of a request: 1 for a small matrix; for a large one a team that grows
@@ -306,6 +358,7 @@ void pbrcm_session::run()
             Request* r = queued.front();
             if (bytes_in_flight + r->dev_bytes > cap_bytes && !running.empty())
                 break;
+            decide_mode(r);
             const int need = choose_ctas(r);
             const int units = r->team && !r->cluster ? need * units_per_sm : need;
             if (ctas_in_use + units > cap_ctas && !running.empty())
@@ -364,6 +417,13 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
         return PBRCM_ERR_OOM;
     s->C = &ctx->ctx;
     cudaSetDevice(s->C->device);
+    {
+        std::lock_guard<std::mutex> lk(s->C->mu);
+        if (s->C->session_pinned)
+            s->pinned_pool = std::static_pointer_cast<PinnedPool>(s->C->session_pinned);
+        else
+            s->C->session_pinned = s->pinned_pool;
+    }
     s->cap_bytes = cfg && cfg->memory_cap_bytes ? cfg->memory_cap_bytes : 120ull * 1000 * 1000 * 1000;
     s->max_inflight = cfg && cfg->max_inflight ? cfg->max_inflight : 4096;
     const uint32_t ns = cfg && cfg->streams ? std::min<uint32_t>(cfg->streams, 128) : 64;
@@ -389,6 +449,8 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
         s->team_max = std::max(s->team_min, std::atoi(e));
     if (const char* e = std::getenv("PBRCM_SESSION_IDLE_TEAM"))
         s->idle_team = std::max(0, std::atoi(e));
+    if (const char* e = std::getenv("PBRCM_SESSION_LIGHT_TEAM_N"))
+        s->light_team_n = (uint32_t)std::max(1L, std::atol(e));
     if (const char* e = std::getenv("PBRCM_SESSION_CLUSTER_MAX"))
         s->cluster_max = std::max(0, std::min(16, std::atoi(e)));
     if (cudaDeviceGetDefaultMemPool(&s->pool, s->C->device) != cudaSuccess) {
@@ -419,9 +481,12 @@ void pbrcm_session_destroy(pbrcm_session* s)
         Request* r = kv.second;
         if (r->ev)
             cudaEventDestroy(r->ev);
-        s->pinned.put(r->host, r->host_cap);
+        if (r->host)
+            s->pinned_pool->put(r->host, r->host_cap);
         delete r;
     }
+    for (cudaEvent_t e : s->free_events)
+        cudaEventDestroy(e);
     for (cudaStream_t st : s->streams) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
@@ -447,11 +512,13 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
         maxdeg = std::max(maxdeg, row_ptr[i + 1] - row_ptr[i]);
     r->maxdeg = maxdeg;
     const int emax_small = kPools[s->small_pool].gemax;
-    r->team = n > s->team_cutoff_n || maxdeg > (uint32_t)emax_small;
-    r->cluster = r->team && s->cluster_max >= 2 && maxdeg <= (uint32_t)emax_small;
-    size_t offs[10];
-    r->dev_bytes = device_bytes(n, nnz, r->team && maxdeg > (uint32_t)kVariants[s->C->team_variant].emax,
-                                r->team ? s->max_ctas : 1, offs);
+    r->big = n > s->team_cutoff_n || maxdeg > (uint32_t)emax_small;
+    r->solo_able = s->C->solo && nnz > 0 && maxdeg <= (uint32_t)emax_small;
+    size_t offs[12];
+    // any request may get a team at admission: room for its words (and hub
+    // scratch for a row longer than the team kernel's chunk)
+    r->dev_bytes = device_bytes(n, nnz, maxdeg > (uint32_t)kVariants[s->C->team_variant].emax, r->solo_able,
+                                s->max_ctas, offs);
     r->d_rp = offs[0];
     r->d_ci = offs[1];
     r->d_node = offs[2];
@@ -462,6 +529,8 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     r->d_cnt = offs[7];
     r->d_agg = offs[8];
     r->d_hub = offs[9];
+    r->d_e2 = offs[10];
+    r->d_gvis = offs[11];
     if (r->dev_bytes > s->cap_bytes) {
         delete r;
         return PBRCM_ERR_BUSY;
@@ -480,9 +549,13 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     {
         std::lock_guard<std::mutex> lk(s->mu);
         cudaSetDevice(s->C->device);
-        r->host = static_cast<unsigned char*>(s->pinned.get(o, r->host_cap));
-        if (!r->host || cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess) {
-            s->pinned.put(r->host, r->host_cap);
+        r->host = static_cast<unsigned char*>(s->pinned_pool->get(o, r->host_cap));
+        if (!s->free_events.empty()) {
+            r->ev = s->free_events.back();
+            s->free_events.pop_back();
+        }
+        if (!r->host || (!r->ev && cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess)) {
+            s->pinned_pool->put(r->host, r->host_cap);
             delete r;
             return PBRCM_ERR_OOM;
         }
@@ -522,18 +595,16 @@ int32_t pbrcm_session_poll(pbrcm_session* s, uint64_t ticket, uint32_t* perm_out
         return PBRCM_OK;
     }
     *done = 1;
-    DevResult res;
-    std::memcpy(&res, r->host + r->off_res, sizeof(res));
+    const DevResult& res = r->res_done;
     if (perm_out && r->rc == PBRCM_OK)
-        std::memcpy(perm_out, r->host + r->off_perm, 4 * (size_t)r->n);
+        std::memcpy(perm_out, r->perm_done.data(), 4 * (size_t)r->n);
     if (result) {
         fill_result(res, r->opt, result);
         result->total_ms = (float)std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
-        result->device_ms = 0.f;
+        // the kernel's own %globaltimer stamps
+        result->device_ms = res.t_end > res.t_begin ? (float)((res.t_end - res.t_begin) * 1e-6) : 0.f;
     }
     int32_t rc = r->rc;
-    cudaEventDestroy(r->ev);
-    s->pinned.put(r->host, r->host_cap);
     s->all.erase(it);
     delete r;
     return rc;

@@ -15,8 +15,10 @@
 //     node an earlier chunk placed is already marked;
 //   * visited is a bitmap in shared memory (n <= kSoloMaxN), so checking a
 //     neighbour costs no global load and marking one no atomic in global
-//     memory; inside a chunk a shared-memory hash keeps the first edge to a
-//     node (atomicMin of the edge index);
+//     memory; a larger matrix keeps the bitmap in global memory (n / 8
+//     bytes, L2-resident: one L2 round trip more per chunk); inside a chunk a
+//     shared-memory hash keeps the first edge to a node (atomicMin of the
+//     edge index);
 //   * every entry's neighbour record -- its column and that column's row
 //     start and valence -- is one 16-byte record of an edge table built once
 //     per matrix (solo_build_edges, during the CSR check), so a chunk needs
@@ -67,9 +69,22 @@ struct Solo {
     SoloSmem<B, EMAX>& s;
     const MatrixView& M;
     const uint4* e2;
+    uint32_t* gvis;  // visited bitmap in global memory (matrices over kSoloMaxN nodes), or nullptr
+    // queue record of position pf_base + (group thread), loaded by the last
+    // form() for the chunk after it (its latency hides behind that chunk);
+    // pf_base == kUnvisited: none
+    uint32_t pf_base = kUnvisited;
+    uint4 pf = make_uint4(0u, 0u, 0u, 0u);
 
-    __device__ __forceinline__ bool visited(uint32_t c) const { return (s.vis[c >> 5] >> (c & 31)) & 1u; }
-    __device__ __forceinline__ void mark(uint32_t c) { atomicOr(&s.vis[c >> 5], 1u << (c & 31)); }
+    __device__ __forceinline__ bool visited(uint32_t c) const
+    {
+        const uint32_t w = gvis ? __ldcg(gvis + (c >> 5)) : s.vis[c >> 5];
+        return (w >> (c & 31)) & 1u;
+    }
+    __device__ __forceinline__ void mark(uint32_t c)
+    {
+        atomicOr(gvis ? gvis + (c >> 5) : &s.vis[c >> 5], 1u << (c & 31));
+    }
 
     // Loads the next chunk's parents from the queue records rec[p .. pend):
     // the longest prefix of at most B parents with at most EMAX edges (every
@@ -81,7 +96,7 @@ struct Solo {
         uint32_t deg = 0;
         const bool have = p + t < pend;
         if (have) {
-            const uint4 r = __ldcg(reinterpret_cast<const uint4*>(M.rec) + p + t);
+            const uint4 r = p == pf_base ? pf : __ldcg(reinterpret_cast<const uint4*>(M.rec) + p + t);
             s.pn[t] = r.x;
             s.prs[t] = r.y;
             s.pdeg[t] = r.z;
@@ -98,6 +113,15 @@ struct Solo {
             s.soff[m] = incl;
             s.m = (uint32_t)m;
             s.Ec = incl;
+        }
+        // the next chunk of this level starts where this one ends: load its
+        // records now
+        const uint32_t nb = p + (uint32_t)m;
+        pf_base = kUnvisited;
+        if (nb < pend) {
+            pf_base = nb;
+            if (nb + t < pend)
+                pf = __ldcg(reinterpret_cast<const uint4*>(M.rec) + nb + t);
         }
         gsync<B>();
         return (uint32_t)m;
@@ -157,16 +181,18 @@ struct Solo {
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
             const uint32_t e = base + lane + 32u * r;
-            cand[r] = false;
-            v[r] = make_uint4(0u, 0u, 0u, 0u);
+            v[r] = make_uint4(kSoloEmpty, 0u, 0u, 0u);
             if (e < Ec) {
                 const uint32_t j = s.epar[e];
                 const uint64_t idx = (uint64_t)s.prs[j] + (e - s.soff[j]);
                 if (PB_CHECK(M.res, idx < M.nnz, 601))
                     v[r] = __ldcg(e2 + idx);
-                cand[r] = PB_CHECK(M.res, v[r].x < M.n, 602) && !visited(v[r].x);
             }
         }
+        // the visited test after all the records are in flight
+#pragma unroll
+        for (int r = 0; r < MAXEPT; ++r)
+            cand[r] = v[r].x != kSoloEmpty && PB_CHECK(M.res, v[r].x < M.n, 602) && !visited(v[r].x);
         // first edge to each unvisited node: insert the node into the table
         // (linear probing; at most EMAX distinct keys in 2 EMAX slots, so a
         // free slot is always found), keep the smallest edge index
@@ -268,6 +294,7 @@ struct Solo {
 template <int B>
 __device__ void solo_build_edges(const MatrixView& M, uint4* e2)
 {
+#pragma unroll 4
     for (uint32_t k = gtid<B>(); k < M.nnz; k += B) {
         const uint32_t c = ld_ro(M.ci + k);
         uint4 r = make_uint4(c, 0u, 0u, 0u);
@@ -290,15 +317,16 @@ __device__ void solo_pass(Solo<B, EMAX>& so, uint32_t start, bool sorted, bool w
     const MatrixView& M = so.M;
     const uint32_t t = gtid<B>();
     const uint32_t words = (M.n + 31u) / 32u;
+    uint32_t* vis = so.gvis ? so.gvis : s.vis;
     for (uint32_t i = t; i < words; i += B)
-        s.vis[i] = 0u;
+        vis[i] = 0u;
     gsync<B>();
     if (t == 0) {
         const uint32_t a = ld_ro(M.rp + start), b = ld_ro(M.rp + start + 1);
         __stcg(reinterpret_cast<uint4*>(M.rec), make_uint4(start, a, b - a, 0u));
         if (write_perm)
             M.perm[reverse ? M.n - 1 : 0] = start;
-        s.vis[start >> 5] |= 1u << (start & 31);
+        so.mark(start);
     }
     gsync<B>();
     uint32_t head = 0, tail = 1, lvl_end = 1, L = 0, lstart = 0;
@@ -336,16 +364,18 @@ __device__ void solo_pass(Solo<B, EMAX>& so, uint32_t start, bool sorted, bool w
 
 // Full reorder of one matrix by one solo group: start search
 // (simple_peripheral.cpp:92-141), the sorted pass, reverse, bandwidth.
-// e2: the matrix's edge records; inv: n words for the inverse permutation.
+// e2: the matrix's edge records; inv: n words for the inverse permutation;
+// gvis: ceil(n / 32) words for the visited bitmap when n > kSoloMaxN (else
+// nullptr: the bitmap is in shared memory).
 template <int B, int EMAX>
 __device__ void solo_reorder(SoloSmem<B, EMAX>& s, const MatrixView& M, const uint4* e2, uint32_t* inv,
-                             const Options& opt)
+                             uint32_t* gvis, const Options& opt)
 {
     const uint32_t t = gtid<B>();
     const uint32_t n = M.n;
     if (t == 0)
         M.res->t_begin = globaltimer();
-    Solo<B, EMAX> so{s, M, e2};
+    Solo<B, EMAX> so{s, M, e2, gvis};
     uint32_t start = opt.start;
     if (start != kUnvisited && start >= n) {
         if (t == 0)

@@ -11,7 +11,7 @@
 //   2. cluster teams for the biggest matrices: CTAs per cluster and how many
 //      matrices get one;
 //   3. the entry count from which a matrix may get a cluster team;
-//   4. serving: the CTA shape of one-CTA requests (512 or 128 threads) and
+//   4. serving: the CTA shape of one-CTA requests (512, 256 or 128 threads) and
 //      the cutoff above which a request runs on a cooperative team instead
 //      (a replay of the batch through a session, all requests at once,
 //      makespan compared).
@@ -65,9 +65,10 @@ pbrcm_tuning from_context(const Context& C)
 
 bool valid(const pbrcm_tuning& t)
 {
-    // the batch kernels' pool shapes 0..3 (4 is the session's one-request CTA)
-    return t.batch_pool <= 3 && t.cluster_size >= 1 && t.cluster_size <= 16 && t.cluster_nnz >= 1 &&
-           t.session_cutoff_n >= 1 && (t.session_pool == 0 || t.session_pool == 4);
+    // the batch kernels' pool shapes 0..3 and 5 (4 is the session's
+    // one-request CTA)
+    return (t.batch_pool <= 3 || t.batch_pool == 5) && t.cluster_size >= 1 && t.cluster_size <= 16 && t.cluster_nnz >= 1 &&
+           t.session_cutoff_n >= 1 && (t.session_pool == 0 || t.session_pool == 4 || t.session_pool == 5);
 }
 
 void to_context(Context& C, const pbrcm_tuning& t)
@@ -290,7 +291,7 @@ int32_t pbrcm_autotune(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t co
         }
     };
     // 1. thread-group shape
-    for (uint32_t p = 0; p <= 3; ++p) {
+    for (uint32_t p : {0u, 1u, 2u, 3u, 5u}) {
         pbrcm_tuning t = best;
         if (p != t.batch_pool) {
             t.batch_pool = p;
@@ -366,7 +367,7 @@ int32_t pbrcm_autotune(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t co
         const uint32_t start_pool = best.session_pool;
         rc = replay(start_cut, start_pool, sdef);
         sbest = sdef;
-        for (uint32_t pool : {0u, 4u})
+        for (uint32_t pool : {0u, 4u, 5u})
             for (uint32_t sh : {16u, 17u, 18u, 19u, 20u}) {
                 const uint32_t cut = 1u << sh;
                 if (rc != PBRCM_OK || (cut == start_cut && pool == start_pool))

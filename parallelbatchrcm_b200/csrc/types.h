@@ -128,6 +128,7 @@ struct BatchJob {
                                   // host-to-device copy after the CSR's copies); nullptr: already there
     uint4* e2;                    // nnz edge records for the one-group engine (solo.cuh), or nullptr
     uint32_t* inv;                // n words (the solo engine's inverse permutation)
+    uint32_t* gvis;               // ceil(n / 32) words: the solo engine's visited bitmap when n > kSoloMaxN
 };
 
 // One entry of the batch work list: member `rank` of job `job`'s team.

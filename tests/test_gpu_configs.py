@@ -91,7 +91,7 @@ def test_mixed_batch_pool_shapes_identical(pbrcm, c4_subset, monkeypatch):
     """Every pool shape (groups per CTA) gives the same permutations."""
     mats, refs = c4_subset
     small = mats[::4]
-    for pool in range(5):
+    for pool in (0, 1, 2, 3, 5):
         monkeypatch.setenv("PBRCM_BATCH_POOL", str(pool))
         ctx = pbrcm.Context(0)
         try:
@@ -99,6 +99,20 @@ def test_mixed_batch_pool_shapes_identical(pbrcm, c4_subset, monkeypatch):
             _check(small, refs[::4], perms, results)
         finally:
             ctx.close()
+
+
+def test_batch_large_matrices_global_visited(pbrcm, gpu_ctx, oracle_mod):
+    """Matrices over 2^18 nodes in a batch: the one-group engine keeps their
+    visited bitmap in global memory (the others in shared memory)."""
+    from parallelbatchrcm_b200 import gen
+    ms = [gen.grid2d(600, 500, seed=41), gen.grid3d(70, 66, 64, seed=42), gen.rgg(400_000, kmin=4, kmax=12, seed=43),
+          gen.grid2d(40, 30, seed=44), gen.grid3d(20, 20, 20, seed=45)]
+    assert sum(m.n > (1 << 18) for m in ms) == 3
+    perms, results = pbrcm.reorder_batch([(m.row_ptr, m.col_idx) for m in ms], reverse=True, ctx=gpu_ctx)
+    for m, p, r in zip(ms, perms, results):
+        ref = oracle_mod.full_reorder(m.row_ptr, m.col_idx, reverse=True)
+        assert r["status"] == 0 and r["start_node"] == ref["start"]
+        assert np.array_equal(p, ref["perm"]) and r["bandwidth"] == ref["bandwidth"]
 
 
 @pytest.fixture(scope="module")
@@ -161,10 +175,14 @@ def test_admission_cap_bounds_bytes_in_flight(pbrcm, gpu_ctx, oracle_mod):
     first has finished; both complete, exactly."""
     from parallelbatchrcm_b200 import gen
     a, b = gen.grid3d(60, 60, 60, seed=6), gen.grid3d(60, 60, 58, seed=7)
-    # the footprint of the larger one (CSR + node table + queue records +
-    # permutation + small words) plus a little, below the two together
-    one = 4 * (a.n + 1) + 4 * a.nnz + 36 * a.n + (1 << 20)
-    sess = pbrcm.Session(gpu_ctx, memory_cap_bytes=one)
+    # the device footprint of the larger one, as the session counts it
+    with pbrcm.Session(gpu_ctx) as probe:
+        t = probe.submit(a.row_ptr, a.col_idx)
+        probe.drain()
+        probe.poll(t)
+        one = probe.stats()["peak_bytes_in_flight"]
+    assert one > 4 * a.nnz
+    sess = pbrcm.Session(gpu_ctx, memory_cap_bytes=one + (one // 4))  # one fits, two do not
     try:
         ta = sess.submit(a.row_ptr, a.col_idx)
         tb = sess.submit(b.row_ptr, b.col_idx)
