@@ -217,8 +217,8 @@ PBRCM_API int32_t pbrcm_reorder_batch_device(pbrcm_context* ctx, const pbrcm_mat
 typedef struct pbrcm_tuning {
     uint32_t batch_pool;       /* thread groups of the batch kernel, one matrix each:
                                   0 = 1 x 512 threads per CTA, 1 = 2 x 256, 2 = 4 x 128,
-                                  3 = 8 x 64, 5 = 256-thread CTAs with 512-edge chunks, three
-                                  per SM */
+                                  3 = 8 x 64, 5 / 6 = 256-thread CTAs with 512 / 1024-edge
+                                  chunks, three per SM */
     uint32_t cluster_size;     /* CTAs of a cluster team for the biggest matrices (1 = none) */
     uint32_t cluster_max;      /* at most this many matrices of a batch get a cluster team */
     uint32_t cluster_nnz;      /* ... and only those with at least this many entries */

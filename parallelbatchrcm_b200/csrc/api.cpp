@@ -177,11 +177,11 @@ int32_t Context::init(int dev)
             tuned = 1;
     }
     batch_pool = env_int("PBRCM_BATCH_POOL", (int)tn.batch_pool);
-    if (batch_pool < 0 || batch_pool > 5 || batch_pool == 4)
+    if (batch_pool < 0 || batch_pool > 6 || batch_pool == 4)
         batch_pool = 1;
     session_cutoff_n = (uint32_t)std::max(1, env_int("PBRCM_SESSION_CUTOFF_N", (int)tn.session_cutoff_n));
     session_pool = env_int("PBRCM_SESSION_POOL", (int)tn.session_pool);
-    if (session_pool != 0 && session_pool != 4 && session_pool != 5)
+    if (session_pool != 0 && session_pool != 4 && session_pool != 5 && session_pool != 6)
         session_pool = 0;
     solo = env_int("PBRCM_SOLO", 1) != 0;
     batch_graphs = env_int("PBRCM_BATCH_GRAPHS", 1) != 0;
@@ -212,7 +212,7 @@ Context::~Context()
             cudaFree(p);
     if (bgraph.exec)
         cudaGraphExecDestroy(bgraph.exec);
-    for (void* p : {(void*)h_jobs, (void*)h_slots, (void*)h_bres})
+    for (void* p : {(void*)h_jobs, (void*)h_slots, (void*)h_bres, (void*)bgraph.h_jobs, (void*)bgraph.h_slots})
         if (p)
             cudaFreeHost(p);
     if (d_ready)

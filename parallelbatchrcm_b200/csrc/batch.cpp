@@ -105,10 +105,11 @@ inline void mix(uint64_t& h, uint64_t v)
 
 // Everything a captured batch depends on: the matrices' buffers and sizes,
 // the options, the shape settings and the context's device buffers.
-uint64_t batch_key(const Context& C, const pbrcm_matrix* mats, uint32_t count, const Options& opt)
+uint64_t batch_key(const Context& C, const pbrcm_matrix* mats, uint32_t count, const Options& opt, bool host)
 {
     uint64_t h = 0x5EED;
     mix(h, count);
+    mix(h, host ? 1 : 2);
     for (uint32_t j = 0; j < count; ++j) {
         mix(h, (uint64_t)(uintptr_t)mats[j].row_ptr);
         mix(h, (uint64_t)(uintptr_t)mats[j].col_idx);
@@ -135,9 +136,10 @@ uint64_t batch_key(const Context& C, const pbrcm_matrix* mats, uint32_t count, c
 // 2. enqueue: zero the per-call words, upload the job list, launch the batch
 //    kernel, then (host buffers) the CSR copies wave by wave on the copy
 //    stream, and the results and permutations back behind the kernel.  A
-//    host-buffer batch whose buffers are all pinned is captured as a CUDA
-//    graph on its first call and replayed on later calls with the same
-//    buffers, options and shape (step 1 is then skipped);
+//    batch on device buffers, or on host buffers that are all pinned, is
+//    captured as a CUDA graph on its first call and replayed on later calls
+//    with the same buffers, sizes, options and shape (step 1 is then
+//    skipped);
 // 3. finish: wait, rerun matrices with a hub row on the team path, fill the
 //    results.
 int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, const pbrcm_options* opts,
@@ -158,10 +160,10 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
     const int maxc = batch_max_ctas(v, C.sms);
     if (maxc <= 0)
         return PBRCM_ERR_CUDA;
-    // graph capture applies to host buffers that are all pinned (a copy from
-    // pageable memory cannot be captured)
-    bool use_graph = host && C.batch_graphs;
-    for (uint32_t j = 0; j < count && use_graph; ++j)
+    // graph capture: device buffers, or host buffers that are all pinned (a
+    // copy from pageable memory cannot be captured)
+    bool use_graph = C.batch_graphs;
+    for (uint32_t j = 0; j < count && use_graph && host; ++j)
         use_graph = is_pinned(mats[j].row_ptr) && (!mats[j].nnz || is_pinned(mats[j].col_idx)) &&
                     is_pinned(mats[j].perm_out);
     // the wait for a wave is bounded; the bound grows with the bytes to copy
@@ -173,7 +175,7 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
     opt.data_wait_ns = opt.wait_ns + (unsigned long long)in_bytes;
     float dms = 0.f;
     bool replayed = false;
-    if (use_graph && C.bgraph.exec && C.bgraph.key == batch_key(C, mats, count, opt) &&
+    if (use_graph && C.bgraph.exec && C.bgraph.key == batch_key(C, mats, count, opt, host) &&
         C.bgraph.order.size() == count) {
         if (cudaGraphLaunch(C.bgraph.exec, st) != cudaSuccess)
             return PBRCM_ERR_CUDA;
@@ -326,11 +328,36 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
         std::memcpy(C.h_jobs, jobs.data(), sizeof(BatchJob) * count);
 
         // ---- enqueue (captured as a graph when use_graph) ----------------
-        if (use_graph && cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-            return PBRCM_ERR_CUDA;
-        bool ok = cudaMemcpyAsync(C.d_jobs, C.h_jobs, sizeof(BatchJob) * count, cudaMemcpyHostToDevice, st) ==
+        // (not on the legacy default stream, nor on a stream the caller is
+        // capturing; a capture that cannot start falls back to plain launches)
+        const BatchJob* src_jobs = C.h_jobs;
+        const BatchSlot* src_slots = C.h_slots;
+        if (use_graph) {
+            // the graph uploads its job list from pinned buffers of its own
+            // (the context's staging is rewritten by every batch that is not
+            // a replay); the graph they belonged to goes first
+            if (C.bgraph.exec) {
+                cudaGraphExecDestroy(C.bgraph.exec);
+                C.bgraph.exec = nullptr;
+            }
+            if (!grow_pinned(C.bgraph.h_jobs, C.bgraph.cap_jobs, count) ||
+                !grow_pinned(C.bgraph.h_slots, C.bgraph.cap_slots, nslots))
+                return PBRCM_ERR_OOM;
+            std::memcpy(C.bgraph.h_jobs, C.h_jobs, sizeof(BatchJob) * count);
+            std::memcpy(C.bgraph.h_slots, C.h_slots, sizeof(BatchSlot) * nslots);
+            src_jobs = C.bgraph.h_jobs;
+            src_slots = C.bgraph.h_slots;
+            cudaStreamCaptureStatus cs_status = cudaStreamCaptureStatusNone;
+            if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread ||
+                cudaStreamIsCapturing(st, &cs_status) != cudaSuccess || cs_status != cudaStreamCaptureStatusNone ||
+                cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                cudaGetLastError();
+                use_graph = false;
+            }
+        }
+        bool ok = cudaMemcpyAsync(C.d_jobs, src_jobs, sizeof(BatchJob) * count, cudaMemcpyHostToDevice, st) ==
                       cudaSuccess &&
-                  cudaMemcpyAsync(C.d_slots, C.h_slots, sizeof(BatchSlot) * nslots, cudaMemcpyHostToDevice, st) ==
+                  cudaMemcpyAsync(C.d_slots, src_slots, sizeof(BatchSlot) * nslots, cudaMemcpyHostToDevice, st) ==
                       cudaSuccess &&
                   (!teamws || cudaMemsetAsync(A + team_off, 0, teamws, st) == cudaSuccess) &&
                   (!nwaves || cudaMemsetAsync(C.d_ready, 0, sizeof(uint32_t) * nwaves, st) == cudaSuccess) &&
@@ -393,10 +420,8 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
             if (g)
                 cudaGraphDestroy(g);
             if (ok) {
-                if (C.bgraph.exec)
-                    cudaGraphExecDestroy(C.bgraph.exec);
                 C.bgraph.exec = exec;
-                C.bgraph.key = batch_key(C, mats, count, opt);
+                C.bgraph.key = batch_key(C, mats, count, opt, host);
                 C.bgraph.order = order;
                 C.bgraph.jobs = jobs;
                 C.bgraph.replays = 0;

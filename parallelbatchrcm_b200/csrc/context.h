@@ -103,10 +103,10 @@ struct Context {
     size_t cap_hslots = 0;
     DevResult* h_bres = nullptr;
     size_t cap_hbres = 0;
-    // host-buffer batches over pinned memory are captured as one CUDA graph
-    // (copies in, kernel, results and permutations out) and replayed while
-    // the same buffers, options and shape come back (PBRCM_BATCH_GRAPHS=0:
-    // never)
+    // batches on device buffers, or on host buffers that are all pinned, are
+    // captured as one CUDA graph (job list and copies in, kernel, results
+    // and permutations out) and replayed while the same buffers, sizes,
+    // options and shape come back (PBRCM_BATCH_GRAPHS=0: never)
     bool batch_graphs = true;
     // serving sessions' pinned staging pool, shared by the context's sessions
     // (created by the first session; type private to session.cpp)
@@ -117,6 +117,11 @@ struct Context {
         std::vector<uint32_t> order;  // job q -> matrix index
         std::vector<BatchJob> jobs;
         uint64_t replays = 0;
+        // the job list the graph uploads (pinned, owned by the graph)
+        BatchJob* h_jobs = nullptr;
+        size_t cap_jobs = 0;
+        BatchSlot* h_slots = nullptr;
+        size_t cap_slots = 0;
     } bgraph;
 
     int32_t init(int dev);

@@ -190,6 +190,7 @@ const PoolInfo kPools[kNumPools] = {
     {512, 2048, 64, 256},
     {128, 512, 128, 512},
     {256, 512, 256, 512},
+    {256, 1024, 256, 1024},
 };
 
 #define PBRCM_DISPATCH(v, CALL)                     \
@@ -201,9 +202,9 @@ const PoolInfo kPools[kNumPools] = {
     }
 
 // the pool shapes' entry points (pool_p<N>.cu, one translation unit each)
-extern const PoolFns kPoolFns0, kPoolFns1, kPoolFns2, kPoolFns3, kPoolFns4, kPoolFns5;
-static const PoolFns* const kPoolTable[kNumPools] = {&kPoolFns0, &kPoolFns1, &kPoolFns2,
-                                                     &kPoolFns3, &kPoolFns4, &kPoolFns5};
+extern const PoolFns kPoolFns0, kPoolFns1, kPoolFns2, kPoolFns3, kPoolFns4, kPoolFns5, kPoolFns6;
+static const PoolFns* const kPoolTable[kNumPools] = {&kPoolFns0, &kPoolFns1, &kPoolFns2, &kPoolFns3,
+                                                     &kPoolFns4, &kPoolFns5, &kPoolFns6};
 
 size_t variant_smem(int v)
 {

@@ -27,7 +27,7 @@ struct PoolInfo {
     int group;
     int gemax;
 };
-constexpr int kNumPools = 6;
+constexpr int kNumPools = 7;
 extern const PoolInfo kPools[kNumPools];
 
 // Entry points of one pool shape (see launch_batch / launch_cluster).

@@ -139,6 +139,7 @@ struct pbrcm_session {
     int cluster_max = 0;
     uint64_t team_nnz = 1ull << 19;
     uint32_t light_team_n = 1u << 14;  // under light load, requests above this many nodes get a team
+    bool big_solo = false;  // under load, big requests run as one solo CTA too (PBRCM_SESSION_BIG_SOLO)
 
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -307,7 +308,7 @@ void pbrcm_session::retire(Request* r)
 void pbrcm_session::decide_mode(Request* r) const
 {
     const bool light = ctas_in_use * 4 < cap_ctas && queued.size() <= 2;
-    r->team = r->big || (light && r->n > light_team_n);
+    r->team = (r->big && (!r->solo_able || !big_solo || light)) || (light && r->n > light_team_n);
     r->solo = !r->team && r->solo_able;
     r->cluster = r->team && cluster_max >= 2 && r->maxdeg <= (uint32_t)kPools[small_pool].gemax;
 }
@@ -449,6 +450,8 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
         s->team_max = std::max(s->team_min, std::atoi(e));
     if (const char* e = std::getenv("PBRCM_SESSION_IDLE_TEAM"))
         s->idle_team = std::max(0, std::atoi(e));
+    if (const char* e = std::getenv("PBRCM_SESSION_BIG_SOLO"))
+        s->big_solo = std::atoi(e) != 0;
     if (const char* e = std::getenv("PBRCM_SESSION_LIGHT_TEAM_N"))
         s->light_team_n = (uint32_t)std::max(1L, std::atol(e));
     if (const char* e = std::getenv("PBRCM_SESSION_CLUSTER_MAX"))

@@ -30,7 +30,8 @@
 // Per chunk: the edge-to-parent map, the edge records, the visited test and
 // the hash insert, a warp-ballot compaction in edge order, the rank of each
 // parent's children by (valence, slot), the writes of the queue records and
-// the permutation, and the visited marks -- six group barriers.
+// the permutation, and the visited marks -- five group barriers in the chunk
+// and three where its parents are formed.
 #pragma once
 
 #include "engine.cuh"
@@ -50,17 +51,27 @@ struct SoloSmem {
     uint32_t soff[B + 1];
     uint32_t cs[B], cc[B];  // first compacted child / child count per parent
     uint32_t epar[EMAX];    // chunk edge -> parent
-    uint32_t hkey[H], hval[H];
-    // the chunk's children in edge order, then their ranked order
-    uint32_t ch_c[EMAX], ch_rs[EMAX], ch_deg[EMAX], ch_par[EMAX];
-    uint32_t so_idx[EMAX];
-    uint32_t wcnt[W];
+    // the dedup table; once the chunk's children are known its room holds
+    // their ranked order (so_idx: rank -> compacted index)
+    union {
+        struct {
+            uint32_t hkey[H], hval[H];
+        };
+        uint32_t so_idx[EMAX];
+    };
+    // the chunk's children in edge order: node, row start, and valence with
+    // the parent's chunk index in the high bits (valence < 2^kParShift)
+    uint32_t ch_c[EMAX], ch_rs[EMAX], ch_dp[EMAX];
+    uint32_t wcnt[W], wdeg[W];
     uint32_t scanbuf[2][W];
     uint32_t tmp32[W + 1];
     unsigned long long tmp64[2 * W + 2];
-    uint32_t m, Ec, Q, Qdeg, carry;
+    uint32_t m, Ec;
     uint32_t bcast[4];
 };
+
+constexpr uint32_t kParShift = 20;  // ch_dp: valence in the low 20 bits, parent index above
+constexpr uint32_t kDegMask = (1u << kParShift) - 1u;
 
 template <int B, int EMAX>
 struct Solo {
@@ -127,18 +138,17 @@ struct Solo {
         return (uint32_t)m;
     }
 
-    // The ranked children of the last chunk become the parents of the next.
-    __device__ void form_from_children()
+    // The Q ranked children of the last chunk become the parents of the next.
+    __device__ void form_from_children(uint32_t Q)
     {
         const uint32_t t = gtid<B>();
-        const uint32_t Q = s.Q;
         uint32_t deg = 0;
         if (t < Q) {
             const uint32_t x = s.so_idx[t];
+            deg = s.ch_dp[x] & kDegMask;
             s.pn[t] = s.ch_c[x];
             s.prs[t] = s.ch_rs[x];
-            s.pdeg[t] = s.ch_deg[x];
-            deg = s.ch_deg[x];
+            s.pdeg[t] = deg;
         }
         uint32_t total;
         const uint32_t excl = block_scan1<B>(deg, total, s.scanbuf[1]);
@@ -155,8 +165,11 @@ struct Solo {
     // One chunk: finds the children of parents [0, m), ranks them (sorted:
     // by valence, stable; else slot order), writes their queue records at
     // positions P.. and, with write_perm, the permutation, and marks them
-    // visited.  Returns the number of children.
-    __device__ uint32_t step(uint32_t P, bool sorted, bool write_perm, bool reverse)
+    // visited.  Returns the number of children; qdeg = their valences' sum.
+    // Ends without a group barrier: the next form() has barriers before
+    // anyone touches this chunk's shared buffers again (the caller adds one
+    // where the next chunk reads the queue records this one wrote).
+    __device__ uint32_t step(uint32_t P, bool sorted, bool write_perm, bool reverse, uint32_t& qdeg)
     {
         const uint32_t t = gtid<B>(), lane = t & 31u, w = t >> 5;
         const uint32_t m = s.m, Ec = s.Ec;
@@ -216,7 +229,7 @@ struct Solo {
         gsync<B>();
         // the winners, compacted in edge order: per warp by ballot, then the
         // warps' counts
-        uint32_t cnt = 0, posr[MAXEPT];
+        uint32_t cnt = 0, posr[MAXEPT], dsum = 0;
         bool win[MAXEPT];
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
@@ -224,16 +237,24 @@ struct Solo {
             const uint32_t bal = __ballot_sync(kFull, win[r]);
             posr[r] = cnt + __popc(bal & ((1u << lane) - 1u));
             cnt += __popc(bal);
+            dsum += win[r] ? v[r].z : 0u;
         }
-        if (lane == 0)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            dsum += __shfl_xor_sync(kFull, dsum, o);
+        if (lane == 0) {
             s.wcnt[w] = cnt;
+            s.wdeg[w] = dsum;
+        }
         gsync<B>();
         uint32_t wbase = 0, Q = 0;
+        qdeg = 0;
 #pragma unroll
         for (int i = 0; i < SoloSmem<B, EMAX>::W; ++i) {
             const uint32_t c = s.wcnt[i];
             wbase += (uint32_t)i < w ? c : 0u;
             Q += c;
+            qdeg += s.wdeg[i];
         }
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
@@ -242,8 +263,7 @@ struct Solo {
                 const uint32_t j = s.epar[base + lane + 32u * r];
                 s.ch_c[x] = v[r].x;
                 s.ch_rs[x] = v[r].y;
-                s.ch_deg[x] = v[r].z;
-                s.ch_par[x] = j;
+                s.ch_dp[x] = v[r].z | (j << kParShift);
                 atomicAdd(&s.cc[j], 1u);
                 atomicMin(&s.cs[j], x);
             }
@@ -251,14 +271,14 @@ struct Solo {
         gsync<B>();
         // rank inside each parent's run: (valence, position) when sorted
         for (uint32_t x = t; x < Q; x += B) {
-            const uint32_t j = s.ch_par[x];
+            const uint32_t j = s.ch_dp[x] >> kParShift;
             const uint32_t st = s.cs[j], len = s.cc[j];
             uint32_t rank = x - st;
             if (sorted && len > 1) {
-                const uint32_t dx = s.ch_deg[x];
+                const uint32_t dx = s.ch_dp[x] & kDegMask;
                 rank = 0;
                 for (uint32_t y = st; y < st + len; ++y) {
-                    const uint32_t dy = s.ch_deg[y];
+                    const uint32_t dy = s.ch_dp[y] & kDegMask;
                     rank += (dy < dx) || (dy == dx && y < x);
                 }
             }
@@ -266,24 +286,17 @@ struct Solo {
         }
         gsync<B>();
         // place: queue records, the permutation, the visited marks
-        uint32_t dsum = 0;
         for (uint32_t i = t; i < Q; i += B) {
             const uint32_t x = s.so_idx[i];
             const uint32_t pos = P + i;
             if (PB_CHECK(M.res, pos < M.n, 603)) {
-                __stcg(reinterpret_cast<uint4*>(M.rec) + pos, make_uint4(s.ch_c[x], s.ch_rs[x], s.ch_deg[x], 0u));
+                __stcg(reinterpret_cast<uint4*>(M.rec) + pos,
+                       make_uint4(s.ch_c[x], s.ch_rs[x], s.ch_dp[x] & kDegMask, 0u));
                 if (write_perm)
                     M.perm[reverse ? M.n - 1 - pos : pos] = s.ch_c[x];
             }
             mark(s.ch_c[x]);
-            dsum += s.ch_deg[x];
         }
-        dsum = block_reduce_sum<B, uint32_t>(dsum, s.tmp32);  // ends with a group barrier
-        if (t == 0) {
-            s.Q = Q;
-            s.Qdeg = dsum;
-        }
-        gsync<B>();
         return Q;
     }
 };
@@ -331,6 +344,7 @@ __device__ void solo_pass(Solo<B, EMAX>& so, uint32_t start, bool sorted, bool w
     gsync<B>();
     uint32_t head = 0, tail = 1, lvl_end = 1, L = 0, lstart = 0;
     bool carry = false;  // the chunk's parents are the last chunk's children, still in shared memory
+    uint32_t q = 0;
     while (head < tail) {
         if (head == lvl_end) {
             L += 1;
@@ -339,18 +353,26 @@ __device__ void solo_pass(Solo<B, EMAX>& so, uint32_t start, bool sorted, bool w
         }
         uint32_t m;
         if (carry) {
-            so.form_from_children();
-            m = s.m;
+            so.form_from_children(q);
+            m = q;
         } else {
             m = so.form(head, lvl_end);
         }
         // a whole level in one chunk whose children fit one chunk: they are
         // the next chunk's parents
         const bool whole_level = head + m == lvl_end && head + m == tail;
-        const uint32_t q = so.step(tail, sorted, write_perm, reverse);
+        uint32_t qdeg = 0;
+        q = so.step(tail, sorted, write_perm, reverse, qdeg);
         head += m;
         tail += q;
-        carry = whole_level && q > 0 && q <= (uint32_t)B && s.Qdeg <= (uint32_t)EMAX;
+        carry = whole_level && q > 0 && q <= (uint32_t)B && qdeg <= (uint32_t)EMAX;
+        // a chunk that ends its level hands its children over through the
+        // queue records it has just written (unless they stay in shared
+        // memory): every thread's records must be in before the next chunk
+        // reads them.  Otherwise the next chunk's parents were written by
+        // earlier chunks, behind barriers already passed.
+        if (head == lvl_end && !carry)
+            gsync<B>();
         if (tail > M.n) {  // cannot happen on a valid run
             if (t == 0)
                 set_status(M.res, kErrCheck, 604);

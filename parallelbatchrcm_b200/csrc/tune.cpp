@@ -67,8 +67,8 @@ bool valid(const pbrcm_tuning& t)
 {
     // the batch kernels' pool shapes 0..3 and 5 (4 is the session's
     // one-request CTA)
-    return (t.batch_pool <= 3 || t.batch_pool == 5) && t.cluster_size >= 1 && t.cluster_size <= 16 && t.cluster_nnz >= 1 &&
-           t.session_cutoff_n >= 1 && (t.session_pool == 0 || t.session_pool == 4 || t.session_pool == 5);
+    return (t.batch_pool <= 3 || t.batch_pool == 5 || t.batch_pool == 6) && t.cluster_size >= 1 && t.cluster_size <= 16 && t.cluster_nnz >= 1 &&
+           t.session_cutoff_n >= 1 && (t.session_pool == 0 || (t.session_pool >= 4 && t.session_pool < (uint32_t)kNumPools));
 }
 
 void to_context(Context& C, const pbrcm_tuning& t)
@@ -291,7 +291,7 @@ int32_t pbrcm_autotune(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t co
         }
     };
     // 1. thread-group shape
-    for (uint32_t p : {0u, 1u, 2u, 3u, 5u}) {
+    for (uint32_t p : {0u, 1u, 2u, 3u, 5u, 6u}) {
         pbrcm_tuning t = best;
         if (p != t.batch_pool) {
             t.batch_pool = p;
@@ -367,7 +367,7 @@ int32_t pbrcm_autotune(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t co
         const uint32_t start_pool = best.session_pool;
         rc = replay(start_cut, start_pool, sdef);
         sbest = sdef;
-        for (uint32_t pool : {0u, 4u, 5u})
+        for (uint32_t pool : {0u, 4u, 5u, 6u})
             for (uint32_t sh : {16u, 17u, 18u, 19u, 20u}) {
                 const uint32_t cut = 1u << sh;
                 if (rc != PBRCM_OK || (cut == start_cut && pool == start_pool))

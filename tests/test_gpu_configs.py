@@ -91,7 +91,7 @@ def test_mixed_batch_pool_shapes_identical(pbrcm, c4_subset, monkeypatch):
     """Every pool shape (groups per CTA) gives the same permutations."""
     mats, refs = c4_subset
     small = mats[::4]
-    for pool in (0, 1, 2, 3, 5):
+    for pool in (0, 1, 2, 3, 5, 6):
         monkeypatch.setenv("PBRCM_BATCH_POOL", str(pool))
         ctx = pbrcm.Context(0)
         try:
@@ -99,6 +99,37 @@ def test_mixed_batch_pool_shapes_identical(pbrcm, c4_subset, monkeypatch):
             _check(small, refs[::4], perms, results)
         finally:
             ctx.close()
+
+
+def test_batch_graph_replay_between_other_batches(pbrcm, c4_subset):
+    """A captured batch (device buffers; pinned host buffers) replayed after
+    other batches of the same context have rewritten its staging: every
+    replay gives the oracle's permutations."""
+    import torch
+    mats, refs = c4_subset
+    a, ra = mats[:48], refs[:48]
+    b = mats[48:96]
+    dev = torch.device("cuda", 0)
+    ctx = pbrcm.Context(0)
+    try:
+        dm = [(torch.from_numpy(rp.view(np.int32)).to(dev), torch.from_numpy(ci.view(np.int32)).to(dev),
+               torch.empty(rp.shape[0] - 1, dtype=torch.int32, device=dev)) for rp, ci in a]
+        pinned = [(torch.from_numpy(rp.view(np.int32)).pin_memory().numpy().view(np.uint32),
+                   torch.from_numpy(ci.view(np.int32)).pin_memory().numpy().view(np.uint32)) for rp, ci in a]
+        outs = [torch.empty(rp.shape[0] - 1, dtype=torch.int32).pin_memory().numpy().view(np.uint32) for rp, _ in a]
+        for rep in range(3):
+            for _, _, p in dm:
+                p.fill_(-1)
+            res = pbrcm.reorder_batch_device(dm, reverse=True, ctx=ctx)  # captured, then replayed
+            _check(a, ra, [p.cpu().numpy() for _, _, p in dm], res)
+            pbrcm.reorder_batch(b, reverse=True, ctx=ctx)  # pageable: plain launches over the staging
+            for o in outs:
+                o.fill(0xFFFFFFFF)
+            perms, res = pbrcm.reorder_batch(pinned, reverse=True, ctx=ctx, perms_out=outs)
+            _check(a, ra, perms, res)
+            pbrcm.reorder_batch(b[: 8 + 8 * rep], reverse=True, ctx=ctx)
+    finally:
+        ctx.close()
 
 
 def test_batch_large_matrices_global_visited(pbrcm, gpu_ctx, oracle_mod):
