@@ -218,7 +218,10 @@ typedef struct pbrcm_tuning {
     uint32_t batch_pool;       /* thread groups of the batch kernel, one matrix each:
                                   0 = 1 x 512 threads per CTA, 1 = 2 x 256, 2 = 4 x 128,
                                   3 = 8 x 64, 5 / 6 = 256-thread CTAs with 512 / 1024-edge
-                                  chunks, three per SM */
+                                  chunks, 7 = 2 x 256 with 2048-edge chunks */
+    uint32_t batch_kernel;     /* 0: the general batch kernel; 1: the solo batch kernel where
+                                  every job is one group's (no teams, no clusters): the
+                                  one-group engine alone, fewer registers, more CTAs per SM */
     uint32_t cluster_size;     /* CTAs of a cluster team for the biggest matrices (1 = none) */
     uint32_t cluster_max;      /* at most this many matrices of a batch get a cluster team */
     uint32_t cluster_nnz;      /* ... and only those with at least this many entries */

@@ -156,14 +156,16 @@ int32_t Context::init(int dev)
     wide_batch_pass = env_int("PBRCM_WIDE_BATCH_PASS", 1) != 0;
     wide_ctas = wide_ctas_per_sm() * sms;
     // batch / serving shape: built-in defaults (measured on the 4,096-matrix
-    // mixed batch with the solo engine: 132 / 106 / 153 ms for 1 x 512,
-    // 2 x 256, 4 x 128 threads per group; without it 212 / 178 / 220 / 382
-    // ms for 1 x 512 .. 8 x 64), or a tuning file written by pbrcm_autotune
-    // for this device shape and library version (PBRCM_TUNING); a PBRCM_*
-    // knob below still overrides a single setting
+    // mixed batch on a B200: the solo batch kernel with three 256-thread
+    // CTAs per SM, 82 ms; 2 x 256 threads per CTA, 86 ms with the solo
+    // kernel and 89-95 ms with the general one; 1 x 512, 102 ms; 2 x 256
+    // with 2,048-edge chunks, 109 ms), or a tuning file written by
+    // pbrcm_autotune for this device shape and library version
+    // (PBRCM_TUNING); a PBRCM_* knob below still overrides a single setting
     pbrcm_tuning tn;
     std::memset(&tn, 0, sizeof(tn));
-    tn.batch_pool = 1;
+    tn.batch_pool = 6;
+    tn.batch_kernel = 1;
     // no cluster teams by default: with the solo engine one group takes even
     // the biggest matrices of the mixed batch faster than a cluster team of
     // the engine does (100 ms against 106 ms for the 4,096-matrix batch)
@@ -177,13 +179,14 @@ int32_t Context::init(int dev)
             tuned = 1;
     }
     batch_pool = env_int("PBRCM_BATCH_POOL", (int)tn.batch_pool);
-    if (batch_pool < 0 || batch_pool > 6 || batch_pool == 4)
-        batch_pool = 1;
+    if (!batch_pool_ok(batch_pool))
+        batch_pool = 6;
     session_cutoff_n = (uint32_t)std::max(1, env_int("PBRCM_SESSION_CUTOFF_N", (int)tn.session_cutoff_n));
     session_pool = env_int("PBRCM_SESSION_POOL", (int)tn.session_pool);
-    if (session_pool != 0 && session_pool != 4 && session_pool != 5 && session_pool != 6)
+    if (!session_pool_ok(session_pool))
         session_pool = 0;
     solo = env_int("PBRCM_SOLO", 1) != 0;
+    batch_solo_kernel = env_int("PBRCM_BATCH_SOLO_KERNEL", (int)tn.batch_kernel) != 0;
     batch_graphs = env_int("PBRCM_BATCH_GRAPHS", 1) != 0;
     if (cudaMalloc(&d_agg, kTeamParts * team_part_bytes(maxc)) != cudaSuccess)
         return PBRCM_ERR_OOM;

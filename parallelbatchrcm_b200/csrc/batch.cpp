@@ -119,7 +119,7 @@ uint64_t batch_key(const Context& C, const pbrcm_matrix* mats, uint32_t count, c
     for (uint64_t v : {(uint64_t)opt.start, (uint64_t)opt.reverse, (uint64_t)opt.want_bw, (uint64_t)opt.outnodes,
                        (uint64_t)opt.wait_ns, (uint64_t)opt.phantom, (uint64_t)C.batch_pool,
                        (uint64_t)C.cluster_size, (uint64_t)C.cluster_max, (uint64_t)C.cluster_nnz,
-                       (uint64_t)C.solo, (uint64_t)(uintptr_t)C.d_arena, (uint64_t)(uintptr_t)C.d_jobs,
+                       (uint64_t)C.solo, (uint64_t)C.batch_solo_kernel, (uint64_t)(uintptr_t)C.d_arena, (uint64_t)(uintptr_t)C.d_jobs,
                        (uint64_t)(uintptr_t)C.d_slots, (uint64_t)(uintptr_t)C.d_bres,
                        (uint64_t)(uintptr_t)C.d_ready, (uint64_t)(uintptr_t)C.d_counter,
                        (uint64_t)(uintptr_t)C.h_bres})
@@ -256,10 +256,10 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
             // for its inverse permutation
             slot[j].e2 = 0;
             slot[j].gvis = 0;
-            if (C.solo && q >= nbig && team[q] == 1 && m.nnz > 0) {
+            if (C.solo && q >= nbig && team[q] == 1 && m.nnz > 0 && m.n <= kSoloMaxNodes) {
                 off = align16(off);
                 slot[j].e2 = off;
-                off += 16 * (size_t)m.nnz;
+                off += 8 * (size_t)m.nnz;
                 if (m.n > kSoloMaxN) {  // the visited bitmap does not fit shared memory
                     slot[j].gvis = off;
                     off = align16(off + 4 * (((size_t)m.n + 31) / 32));
@@ -313,7 +313,7 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
             J.M.res = C.d_bres + q;
             J.team = q < nbig ? 1 : team[q];
             J.ready = host ? C.d_ready + wave[q] : nullptr;
-            J.e2 = slot[j].e2 ? reinterpret_cast<uint4*>(A + slot[j].e2) : nullptr;
+            J.e2 = slot[j].e2 ? reinterpret_cast<uint2*>(A + slot[j].e2) : nullptr;
             J.gvis = slot[j].gvis ? reinterpret_cast<uint32_t*>(A + slot[j].gvis) : nullptr;
             J.inv = reinterpret_cast<uint32_t*>(A + slot[j].node);
             if (team[q] > 1) {
@@ -376,10 +376,14 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
             ok = launch_cluster(v, C.d_jobs, nbig, C.d_slots, (uint32_t)nslots, C.d_counter, copt, opt,
                                 C.cluster_size, ncl, st) == cudaSuccess;
         } else if (ok) {
+            // every job one group's: the solo batch kernel where the shape
+            // has one, else the general kernel
             const uint32_t per = (uint32_t)(kPools[v].block / kPools[v].group);
-            const int ctas = std::max(1, std::min<int>(maxc, (int)((nslots + per - 1) / per)));
-            ok = launch_batch(v, C.d_jobs, C.d_slots, (uint32_t)nslots, C.d_counter, opt, ctas, cooperative, st) ==
-                 cudaSuccess;
+            const int smaxc = C.solo && C.batch_solo_kernel && !cooperative ? solo_max_ctas(v, C.sms) : 0;
+            const int ctas = std::max(1, std::min<int>(smaxc > 0 ? smaxc : maxc, (int)((nslots + per - 1) / per)));
+            ok = (smaxc > 0 ? launch_solo(v, C.d_jobs, C.d_slots, (uint32_t)nslots, C.d_counter, opt, ctas, st)
+                            : launch_batch(v, C.d_jobs, C.d_slots, (uint32_t)nslots, C.d_counter, opt, ctas,
+                                           cooperative, st)) == cudaSuccess;
         }
         if (ok && host) {
             // the inputs, wave by wave, each wave's ready word after its CSRs

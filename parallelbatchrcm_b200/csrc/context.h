@@ -21,8 +21,12 @@ struct Context {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int team_variant = 1;   // kernel shape of the one-matrix team
     int team_ctas = 0;      // CTAs of the one-matrix team
-    int batch_pool = 1;     // shape of the batch kernels (kPools: CTA and group sizes)
+    int batch_pool = 6;     // shape of the batch kernels (kPools: CTA and group sizes)
     bool solo = true;       // batch: one-group jobs run the solo engine where it applies (PBRCM_SOLO=0: never)
+    // batch without teams: the solo batch kernel (no team engine code, fewer
+    // registers, more CTAs per SM) in place of the general one
+    // (PBRCM_BATCH_SOLO_KERNEL=0: never)
+    bool batch_solo_kernel = true;
     uint32_t solo_edges = 0;    // levels at most this big run on one CTA
     uint32_t solo_parents = 0;
     uint32_t barrier = 0;       // team barrier implementation

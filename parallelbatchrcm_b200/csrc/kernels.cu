@@ -191,6 +191,7 @@ const PoolInfo kPools[kNumPools] = {
     {128, 512, 128, 512},
     {256, 512, 256, 512},
     {256, 1024, 256, 1024},
+    {512, 2048, 256, 2048},
 };
 
 #define PBRCM_DISPATCH(v, CALL)                     \
@@ -202,9 +203,19 @@ const PoolInfo kPools[kNumPools] = {
     }
 
 // the pool shapes' entry points (pool_p<N>.cu, one translation unit each)
-extern const PoolFns kPoolFns0, kPoolFns1, kPoolFns2, kPoolFns3, kPoolFns4, kPoolFns5, kPoolFns6;
+extern const PoolFns kPoolFns0, kPoolFns1, kPoolFns2, kPoolFns3, kPoolFns4, kPoolFns5, kPoolFns6, kPoolFns7;
 static const PoolFns* const kPoolTable[kNumPools] = {&kPoolFns0, &kPoolFns1, &kPoolFns2, &kPoolFns3,
-                                                     &kPoolFns4, &kPoolFns5, &kPoolFns6};
+                                                     &kPoolFns4, &kPoolFns5, &kPoolFns6, &kPoolFns7};
+
+bool batch_pool_ok(int p)
+{
+    return p >= 0 && p < kNumPools && p != 4;
+}
+
+bool session_pool_ok(int p)
+{
+    return p >= 0 && p < kNumPools && kPools[p].block == kPools[p].group;
+}
 
 size_t variant_smem(int v)
 {
@@ -225,6 +236,19 @@ int team_max_ctas(int v, int sms)
 int batch_max_ctas(int p, int sms)
 {
     return p >= 0 && p < kNumPools ? kPoolTable[p]->batch_max_ctas(sms) : 0;
+}
+
+int solo_max_ctas(int p, int sms)
+{
+    return p >= 0 && p < kNumPools ? kPoolTable[p]->solo_max_ctas(sms) : 0;
+}
+
+cudaError_t launch_solo(int p, const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
+                        const Options& opt, int ctas, cudaStream_t st)
+{
+    if (p < 0 || p >= kNumPools)
+        return cudaErrorInvalidValue;
+    return kPoolTable[p]->solo(jobs, slots, nslots, counter, opt, ctas, st);
 }
 
 cudaError_t launch_team(int v, const MatrixView& M, const Options& opt, GridSync* gs, unsigned long long* agg,

@@ -27,8 +27,12 @@ struct PoolInfo {
     int group;
     int gemax;
 };
-constexpr int kNumPools = 7;
+constexpr int kNumPools = 8;
 extern const PoolInfo kPools[kNumPools];
+// Shapes a batch may use (all but 4, the session's 128-thread CTA) and
+// shapes a session may give a one-request CTA (one group per CTA).
+bool batch_pool_ok(int p);
+bool session_pool_ok(int p);
 
 // Entry points of one pool shape (see launch_batch / launch_cluster).
 struct PoolFns {
@@ -39,11 +43,19 @@ struct PoolFns {
     cudaError_t (*cluster)(const BatchJob* jobs, uint32_t nbig, const BatchSlot* slots, uint32_t nslots,
                            uint32_t* counters, const Options& copt, const Options& opt, int csize, int nclusters,
                            cudaStream_t st);
+    int (*solo_max_ctas)(int sms);
+    cudaError_t (*solo)(const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
+                        const Options& opt, int ctas, cudaStream_t st);
 };
 
 size_t variant_smem(int v);
 int team_max_ctas(int v, int sms);   // co-resident CTAs of the team kernel
 int batch_max_ctas(int p, int sms);  // co-resident CTAs of pool p's batch kernel
+// Pool p's solo batch kernel (only one-group jobs with edge records, no
+// teams): co-resident CTAs (0: the shape has none) and the launch.
+int solo_max_ctas(int p, int sms);
+cudaError_t launch_solo(int p, const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
+                        const Options& opt, int ctas, cudaStream_t st);
 
 cudaError_t launch_validate(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint32_t nnz, DevResult* res,
                             int sms, cudaStream_t st);

@@ -91,7 +91,8 @@ __device__ void group_take_slots(unsigned char* raw, const BatchJob* jobs, const
             // one group alone on a matrix whose rows fit a chunk: the solo
             // engine (visited bitmap in shared memory, or in global memory
             // for a matrix over kSoloMaxN nodes)
-            if (job.e2 != nullptr && job.team == 1 && (job.M.n <= kSoloMaxN || job.gvis != nullptr) &&
+            if (job.e2 != nullptr && job.team == 1 && job.M.n <= kSoloMaxNodes &&
+                (job.M.n <= kSoloMaxN || job.gvis != nullptr) &&
                 read_status(job.M.res) == 0 && __ldcg(&job.M.res->maxdeg) <= (uint32_t)GE) {
                 solo_reorder<GB, GE>(*reinterpret_cast<SoloSmem<GB, GE>*>(raw), job.M, job.e2, job.inv,
                                      job.M.n > kSoloMaxN ? job.gvis : nullptr, opt);
@@ -116,6 +117,71 @@ __device__ void group_take_slots(unsigned char* raw, const BatchJob* jobs, const
         reorder_matrix<GB, GE>(s, job.M, team, job.words, opt);
         gsync<GB>();
     }
+}
+
+// Bytes of one group's shared memory in the solo batch kernel.
+template <int GB, int GE>
+__host__ __device__ constexpr size_t solo_stride()
+{
+    return (sizeof(SoloSmem<GB, GE>) + 127) & ~(size_t)127;
+}
+
+// One thread group's share of a batch in which every job is a one-group job
+// with edge records (no teams, no clusters): the solo engine alone, so the
+// kernel carries none of the team engine's registers.  A matrix with a row
+// longer than a chunk is left to the host's rerun on the team path
+// (kNeedHub), as the general kernel does.
+template <int GB, int GE>
+__device__ void group_take_solo(unsigned char* raw, const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots,
+                                uint32_t* counter, const Options& opt)
+{
+    auto& s = *reinterpret_cast<SoloSmem<GB, GE>*>(raw);
+    const uint32_t t = gtid<GB>();
+    while (true) {
+        if (t == 0)
+            s.bcast[0] = atomicAdd(counter, 1u);
+        gsync<GB>();
+        const uint32_t slot = s.bcast[0];
+        gsync<GB>();
+        if (slot >= nslots)
+            break;
+        const BatchJob job = jobs[slots[slot].job];
+        if (job.ready != nullptr) {
+            wait_ready<GB>(job.ready, opt.data_wait_ns, job.M.res, reinterpret_cast<int*>(&s.bcast[1]));
+            const bool arrived = s.bcast[1] != 0;
+            gsync<GB>();  // everyone has read bcast[1] before it is written again
+            if (!arrived)
+                continue;
+        }
+        validate_group<GB>(job.M, s.tmp32);
+        if (read_status(job.M.res) != 0)
+            continue;
+        // rows longer than a chunk, or no room for edge records (the host
+        // gives a matrix of more than kSoloMaxNodes nodes none): the host
+        // reruns the matrix on the team path
+        if (__ldcg(&job.M.res->maxdeg) > (uint32_t)GE || (job.e2 == nullptr && job.M.nnz > 0) ||
+            (job.M.n > kSoloMaxN && job.gvis == nullptr)) {
+            if (t == 0)
+                set_status(job.M.res, kNeedHub, 0);
+            continue;
+        }
+        solo_build_edges<GB>(job.M, job.e2);
+        gsync<GB>();
+        solo_reorder<GB, GE>(s, job.M, job.e2, job.inv, job.M.n > kSoloMaxN ? job.gvis : nullptr, opt);
+        gsync<GB>();
+    }
+}
+
+// The solo batch kernel: CTAs of B threads split into B / GB groups, each
+// reordering one matrix at a time with the solo engine (compiled for MINB
+// CTAs per SM).
+template <int B, int GB, int GE, int MINB>
+__global__ void __launch_bounds__(B, MINB) k_solo_batch(const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots,
+                                                        uint32_t* counter, Options opt)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    group_take_solo<GB, GE>(smem_raw + (threadIdx.x / GB) * solo_stride<GB, GE>(), jobs, slots, nslots, counter,
+                            opt);
 }
 
 // Many matrices in one launch.  A CTA of B threads runs B / GB independent
@@ -204,8 +270,9 @@ namespace {
 // The batch kernels of one pool shape: CTAs of B threads (cluster teams of
 // whole CTAs, EMAX edges per chunk), split into groups of GB threads (GE
 // edges per chunk) for the one-group slots; MINB CTAs per SM (the register
-// bound the kernels are compiled for).
-template <int B, int EMAX, int GB, int GE, int MINB>
+// bound the kernels are compiled for); the solo batch kernel of the same
+// groups for SMINB CTAs per SM (0: none for this shape).
+template <int B, int EMAX, int GB, int GE, int MINB, int SMINB>
 struct Pool {
     static_assert(B % GB == 0 && B / GB <= 15, "at most 15 groups (named barriers 1..15) per CTA");
     static size_t batch_smem() { return (size_t)(B / GB) * group_stride<B, GB, GE>(); }
@@ -266,6 +333,47 @@ struct Pool {
         return cudaLaunchKernelEx(&cfg, k_reorder_cluster<B, EMAX, GB, GE, MINB>, jobs, nbig, slots, nslots, counters, copt,
                                   opt);
     }
+    static constexpr bool kSolo = SMINB > 0 && (size_t)(B / GB) * solo_stride<GB, GE>() <= (size_t)226 * 1024;
+    static size_t solo_smem() { return (size_t)(B / GB) * solo_stride<GB, GE>(); }
+    static const void* solo_fn()
+    {
+        if constexpr (kSolo)
+            return (const void*)k_solo_batch<B, GB, GE, (SMINB > 0 ? SMINB : 1)>;
+        return nullptr;
+    }
+    static cudaError_t solo_prepare()
+    {
+        static cudaError_t once = [] {
+            if (!kSolo)
+                return cudaErrorInvalidValue;
+            return cudaFuncSetAttribute(solo_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solo_smem());
+        }();
+        return once;
+    }
+    static int solo_max_ctas(int sms)
+    {
+        if (solo_prepare() != cudaSuccess)
+            return 0;
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, solo_fn(), B, solo_smem()) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        return nb * sms;
+    }
+    static cudaError_t solo(const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
+                            const Options& opt, int ctas, cudaStream_t st)
+    {
+        if constexpr (kSolo) {
+            cudaError_t e = solo_prepare();
+            if (e != cudaSuccess)
+                return e;
+            k_solo_batch<B, GB, GE, (SMINB > 0 ? SMINB : 1)><<<ctas, B, solo_smem(), st>>>(jobs, slots, nslots,
+                                                                                           counter, opt);
+            return cudaGetLastError();
+        }
+        return cudaErrorInvalidValue;
+    }
     static int batch_max_ctas(int sms)
     {
         if (prepare() != cudaSuccess)
@@ -302,9 +410,10 @@ struct Pool {
 
 }  // namespace pbrcm
 
-#define PBRCM_DEFINE_POOL(IDX, B, EMAX, GB, GE, MINB)                                                       \
+#define PBRCM_DEFINE_POOL(IDX, B, EMAX, GB, GE, MINB, SMINB)                                                \
     namespace pbrcm {                                                                                       \
     extern const PoolFns kPoolFns##IDX = {                                                                  \
-        &Pool<B, EMAX, GB, GE, MINB>::batch_max_ctas, &Pool<B, EMAX, GB, GE, MINB>::cluster_max_active,     \
-        &Pool<B, EMAX, GB, GE, MINB>::batch, &Pool<B, EMAX, GB, GE, MINB>::cluster};                        \
+        &Pool<B, EMAX, GB, GE, MINB, SMINB>::batch_max_ctas, &Pool<B, EMAX, GB, GE, MINB, SMINB>::cluster_max_active, \
+        &Pool<B, EMAX, GB, GE, MINB, SMINB>::batch, &Pool<B, EMAX, GB, GE, MINB, SMINB>::cluster,                    \
+        &Pool<B, EMAX, GB, GE, MINB, SMINB>::solo_max_ctas, &Pool<B, EMAX, GB, GE, MINB, SMINB>::solo};             \
     }

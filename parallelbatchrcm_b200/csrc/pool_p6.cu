@@ -2,4 +2,4 @@
 // (the solo engine's shared memory packed to 72 KB, 80 registers).
 #include "pool.cuh"
 
-PBRCM_DEFINE_POOL(6, 256, 1024, 256, 1024, 3)
+PBRCM_DEFINE_POOL(6, 256, 1024, 256, 1024, 3, 3)

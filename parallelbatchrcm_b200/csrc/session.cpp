@@ -196,7 +196,7 @@ size_t device_bytes(uint32_t n, uint64_t nnz, bool hub, bool solo, int team_ctas
         o = align16(o + 16 * std::max<uint64_t>(nnz, 1));
     offs[10] = o;  // the solo engine's edge records
     if (solo)
-        o = align16(o + 16 * std::max<uint64_t>(nnz, 1));
+        o = align16(o + 8 * std::max<uint64_t>(nnz, 1));
     offs[11] = o;  // its visited bitmap, when it does not fit shared memory
     if (solo && n > kSoloMaxN)
         o = align16(o + 4 * (((size_t)n + 31) / 32));
@@ -228,7 +228,7 @@ bool pbrcm_session::launch(Request* r)
     J.M = M;
     J.team = 1;
     if (r->solo) {
-        J.e2 = reinterpret_cast<uint4*>(D + r->d_e2);
+        J.e2 = reinterpret_cast<uint2*>(D + r->d_e2);
         J.inv = reinterpret_cast<uint32_t*>(D + r->d_node);
         J.gvis = r->n > kSoloMaxN ? reinterpret_cast<uint32_t*>(D + r->d_gvis) : nullptr;
     }
@@ -516,7 +516,7 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     r->maxdeg = maxdeg;
     const int emax_small = kPools[s->small_pool].gemax;
     r->big = n > s->team_cutoff_n || maxdeg > (uint32_t)emax_small;
-    r->solo_able = s->C->solo && nnz > 0 && maxdeg <= (uint32_t)emax_small;
+    r->solo_able = s->C->solo && nnz > 0 && maxdeg <= (uint32_t)emax_small && n <= kSoloMaxNodes;
     size_t offs[12];
     // any request may get a team at admission: room for its words (and hub
     // scratch for a row longer than the team kernel's chunk)

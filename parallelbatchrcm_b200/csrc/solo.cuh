@@ -20,18 +20,21 @@
 //     shared-memory hash keeps the first edge to a node (atomicMin of the
 //     edge index);
 //   * every entry's neighbour record -- its column and that column's row
-//     start and valence -- is one 16-byte record of an edge table built once
+//     start and valence -- is one 8-byte record of an edge table built once
 //     per matrix (solo_build_edges, during the CSR check), so a chunk needs
 //     one dependent global load per edge (coalesced along each row) instead
-//     of a column load followed by a node-table load;
+//     of a column load followed by a node-table load; the queue holds the
+//     same 8-byte records (node and valence in one word, row start in the
+//     other: n <= kSoloMaxNodes, valences < 4,096);
 //   * the children of a chunk that is a whole level, if they fit one chunk,
 //     stay in shared memory as the next chunk's parents.
 //
-// Per chunk: the edge-to-parent map, the edge records, the visited test and
-// the hash insert, a warp-ballot compaction in edge order, the rank of each
-// parent's children by (valence, slot), the writes of the queue records and
-// the permutation, and the visited marks -- five group barriers in the chunk
-// and three where its parents are formed.
+// Per chunk: each edge's parent by a binary search of the parents' edge
+// offsets, the edge records, the visited test and the dedup-table insert, a
+// warp-ballot compaction in edge order, the rank of each parent's children
+// by (valence, slot), the writes of the queue records and the permutation,
+// and the visited marks -- four group barriers in the chunk and three where
+// its parents are formed.
 #pragma once
 
 #include "engine.cuh"
@@ -49,16 +52,12 @@ struct SoloSmem {
     // parents of the chunk
     uint32_t pn[B], prs[B], pdeg[B];
     uint32_t soff[B + 1];
-    uint32_t cs[B], cc[B];  // first compacted child / child count per parent
-    uint32_t epar[EMAX];    // chunk edge -> parent
-    // the dedup table; once the chunk's children are known its room holds
-    // their ranked order (so_idx: rank -> compacted index)
-    union {
-        struct {
-            uint32_t hkey[H], hval[H];
-        };
-        uint32_t so_idx[EMAX];
-    };
+    uint32_t cs[B], cc[B];  // first compacted child / child count per parent (clear between chunks)
+    // the dedup table: (node << kEdgeBits | chunk edge) of the first edge to
+    // each unvisited node of the chunk; kSoloEmpty where free (clear between
+    // chunks)
+    uint32_t tab[H];
+    uint32_t so_idx[EMAX];  // the children's ranked order: rank -> compacted index
     // the chunk's children in edge order: node, row start, and valence with
     // the parent's chunk index in the high bits (valence < 2^kParShift)
     uint32_t ch_c[EMAX], ch_rs[EMAX], ch_dp[EMAX];
@@ -70,22 +69,51 @@ struct SoloSmem {
     uint32_t bcast[4];
 };
 
+// Chunk edge indices take kEdgeBits bits below the node in a dedup word
+// (nodes < 2^20, chunks of at most 2,048 edges: 31 bits).
+constexpr uint32_t kEdgeBits = 11;
 constexpr uint32_t kParShift = 20;  // ch_dp: valence in the low 20 bits, parent index above
 constexpr uint32_t kDegMask = (1u << kParShift) - 1u;
+
+// Edge and queue records of the solo engine: (node | valence << 20, row
+// start).  A record word never equals kSoloEmpty (valences stay below 4,096).
+constexpr uint32_t kRecNodeBits = 20;
+constexpr uint32_t kRecNodeMask = (1u << kRecNodeBits) - 1u;
+__device__ __forceinline__ uint2 solo_rec(uint32_t node, uint32_t deg, uint32_t rs)
+{
+    return make_uint2(node | (deg << kRecNodeBits), rs);
+}
+__device__ __forceinline__ uint32_t rec_node(uint2 r) { return r.x & kRecNodeMask; }
+__device__ __forceinline__ uint32_t rec_deg(uint2 r) { return r.x >> kRecNodeBits; }
+
+// Requests the lines of e2[rs .. rs + deg) into L2 (at most four 128-byte
+// lines: the rows the engine chunks are short), without waiting.
+__device__ __forceinline__ void prefetch_row(const uint2* e2, uint32_t rs, uint32_t deg)
+{
+    if (deg == 0)
+        return;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(e2 + rs) & ~(uintptr_t)127;
+    const uintptr_t z = reinterpret_cast<uintptr_t>(e2 + rs + deg - 1) & ~(uintptr_t)127;
+    for (uintptr_t l = a; l <= z && l < a + 4 * 128; l += 128)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(l));
+}
 
 template <int B, int EMAX>
 struct Solo {
     static constexpr int MAXEPT = EMAX / B;
     static_assert(EMAX % B == 0 && (EMAX & (EMAX - 1)) == 0, "EMAX: a power of two, a multiple of B");
+    static_assert(EMAX <= (1 << kEdgeBits), "a chunk edge index fits the dedup word");
     SoloSmem<B, EMAX>& s;
     const MatrixView& M;
-    const uint4* e2;
+    const uint2* e2;
+    uint2* q;  // the queue: rec[] of the matrix as 8-byte records
     uint32_t* gvis;  // visited bitmap in global memory (matrices over kSoloMaxN nodes), or nullptr
     // queue record of position pf_base + (group thread), loaded by the last
     // form() for the chunk after it (its latency hides behind that chunk);
     // pf_base == kUnvisited: none
     uint32_t pf_base = kUnvisited;
-    uint4 pf = make_uint4(0u, 0u, 0u, 0u);
+    uint2 pf = make_uint2(0u, 0u);
+    bool pf_ok = false;  // this thread holds a record in pf
 
     __device__ __forceinline__ bool visited(uint32_t c) const
     {
@@ -107,11 +135,11 @@ struct Solo {
         uint32_t deg = 0;
         const bool have = p + t < pend;
         if (have) {
-            const uint4 r = p == pf_base ? pf : __ldcg(reinterpret_cast<const uint4*>(M.rec) + p + t);
-            s.pn[t] = r.x;
+            const uint2 r = p == pf_base ? pf : __ldcg(q + p + t);
+            deg = rec_deg(r);
+            s.pn[t] = rec_node(r);
             s.prs[t] = r.y;
-            s.pdeg[t] = r.z;
-            deg = r.z;
+            s.pdeg[t] = deg;
         }
         uint32_t total;
         const uint32_t excl = block_scan1<B>(deg, total, s.scanbuf[0]);
@@ -129,13 +157,35 @@ struct Solo {
         // records now
         const uint32_t nb = p + (uint32_t)m;
         pf_base = kUnvisited;
+        pf_ok = false;
         if (nb < pend) {
             pf_base = nb;
-            if (nb + t < pend)
-                pf = __ldcg(reinterpret_cast<const uint4*>(M.rec) + nb + t);
+            if (nb + t < pend) {
+                pf = __ldcg(q + nb + t);
+                pf_ok = true;
+            }
         }
         gsync<B>();
         return (uint32_t)m;
+    }
+
+    // next_peripheral_start (engine.cuh) over this queue's 8-byte records:
+    // among the last min(outnodes, n-1) positions, those on the last level;
+    // the last of minimal valence.  One thread.
+    __device__ uint32_t next_start(uint32_t outnodes, uint32_t last_start) const
+    {
+        const uint32_t n = M.n;
+        uint32_t lo = n - min(outnodes, n - 1);
+        lo = max(lo, max(last_start, 1u));
+        uint32_t best = 0, bestdeg = kUnvisited;
+        for (uint32_t pos = lo; pos < n; ++pos) {
+            const uint2 r = __ldcg(q + pos);
+            if (rec_deg(r) <= bestdeg) {
+                bestdeg = rec_deg(r);
+                best = rec_node(r);
+            }
+        }
+        return best;
     }
 
     // The Q ranked children of the last chunk become the parents of the next.
@@ -166,64 +216,72 @@ struct Solo {
     // by valence, stable; else slot order), writes their queue records at
     // positions P.. and, with write_perm, the permutation, and marks them
     // visited.  Returns the number of children; qdeg = their valences' sum.
-    // Ends without a group barrier: the next form() has barriers before
-    // anyone touches this chunk's shared buffers again (the caller adds one
-    // where the next chunk reads the queue records this one wrote).
+    // Four group barriers.  Ends without one: the next form() has barriers
+    // before anyone touches this chunk's shared buffers again (the caller
+    // adds one where the next chunk reads the queue records this one
+    // wrote).  Leaves the dedup table and the parent counters clear.
     __device__ uint32_t step(uint32_t P, bool sorted, bool write_perm, bool reverse, uint32_t& qdeg)
     {
         const uint32_t t = gtid<B>(), lane = t & 31u, w = t >> 5;
         const uint32_t m = s.m, Ec = s.Ec;
-        // edge -> parent map, parent counters, an empty dedup table
-        for (uint32_t j = t; j < m; j += B) {
-            for (uint32_t e = s.soff[j]; e < s.soff[j + 1]; ++e)
-                s.epar[e] = j;
-            s.cs[j] = kSoloEmpty;
-            s.cc[j] = 0;
-        }
-        for (uint32_t i = t; i < (uint32_t)SoloSmem<B, EMAX>::H; i += B) {
-            s.hkey[i] = kSoloEmpty;
-            s.hval[i] = kSoloEmpty;
-        }
-        gsync<B>();
         // warp w owns edges [w * 32 * MAXEPT, ...); lane l takes e = base +
         // l + 32 r, so that a warp reads consecutive records of a row
         const uint32_t base = w * 32u * MAXEPT;
-        uint4 v[MAXEPT];
-        uint32_t slot[MAXEPT];
+        uint2 v[MAXEPT];
+        uint32_t par[MAXEPT], slot[MAXEPT];
         bool cand[MAXEPT];
+        // each edge's parent (the last j < m with soff[j] <= e: a binary
+        // search of fixed depth, the edges' searches side by side; a parent
+        // of valence 0 owns no edge), then the edge's record
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
             const uint32_t e = base + lane + 32u * r;
-            v[r] = make_uint4(kSoloEmpty, 0u, 0u, 0u);
+            uint32_t lo = 0;
+#pragma unroll
+            for (uint32_t d = (uint32_t)B / 2u; d > 0; d >>= 1) {
+                const uint32_t mid = lo + d;
+                if (mid < m && s.soff[mid] <= e)
+                    lo = mid;
+            }
+            par[r] = lo;
+            v[r] = make_uint2(kSoloEmpty, 0u);
             if (e < Ec) {
-                const uint32_t j = s.epar[e];
-                const uint64_t idx = (uint64_t)s.prs[j] + (e - s.soff[j]);
+                const uint64_t idx = (uint64_t)s.prs[lo] + (e - s.soff[lo]);
                 if (PB_CHECK(M.res, idx < M.nnz, 601))
                     v[r] = __ldcg(e2 + idx);
             }
         }
+        // the next chunk's rows into L2 while these records are in flight
+        // (its queue records came with the last form())
+        if (pf_ok)
+            prefetch_row(e2, pf.y, rec_deg(pf));
         // the visited test after all the records are in flight
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r)
-            cand[r] = v[r].x != kSoloEmpty && PB_CHECK(M.res, v[r].x < M.n, 602) && !visited(v[r].x);
-        // first edge to each unvisited node: insert the node into the table
-        // (linear probing; at most EMAX distinct keys in 2 EMAX slots, so a
-        // free slot is always found), keep the smallest edge index
+            cand[r] = v[r].x != kSoloEmpty && PB_CHECK(M.res, rec_node(v[r]) < M.n, 602) && !visited(rec_node(v[r]));
+        // first edge to each unvisited node: (node, edge) in one word, so
+        // that the word's minimum under a fixed node is the first edge; the
+        // node's slot by linear probing (at most EMAX distinct nodes in 2
+        // EMAX slots: a free slot is always found)
         constexpr uint32_t mask = (uint32_t)SoloSmem<B, EMAX>::H - 1u;
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
             slot[r] = 0;
             if (cand[r]) {
-                const uint32_t c = v[r].x;
+                const uint32_t c = rec_node(v[r]);
+                const uint32_t key = (c << kEdgeBits) | (base + lane + 32u * r);
                 uint32_t h = (c * 2654435761u) & mask;
                 while (true) {
-                    const uint32_t k = atomicCAS(&s.hkey[h], kSoloEmpty, c);
-                    if (k == kSoloEmpty || k == c)
+                    const uint32_t old = atomicCAS(&s.tab[h], kSoloEmpty, key);
+                    if (old == kSoloEmpty)
                         break;
+                    if ((old >> kEdgeBits) == c) {
+                        atomicMin(&s.tab[h], key);
+                        break;
+                    }
                     h = (h + 1u) & mask;
                 }
                 slot[r] = h;
-                atomicMin(&s.hval[h], base + lane + 32u * r);
             }
         }
         gsync<B>();
@@ -233,11 +291,11 @@ struct Solo {
         bool win[MAXEPT];
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
-            win[r] = cand[r] && s.hval[slot[r]] == base + lane + 32u * r;
+            win[r] = cand[r] && s.tab[slot[r]] == ((rec_node(v[r]) << kEdgeBits) | (base + lane + 32u * r));
             const uint32_t bal = __ballot_sync(kFull, win[r]);
             posr[r] = cnt + __popc(bal & ((1u << lane) - 1u));
             cnt += __popc(bal);
-            dsum += win[r] ? v[r].z : 0u;
+            dsum += win[r] ? rec_deg(v[r]) : 0u;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
@@ -260,10 +318,10 @@ struct Solo {
         for (int r = 0; r < MAXEPT; ++r) {
             if (win[r]) {
                 const uint32_t x = wbase + posr[r];
-                const uint32_t j = s.epar[base + lane + 32u * r];
-                s.ch_c[x] = v[r].x;
+                const uint32_t j = par[r];
+                s.ch_c[x] = rec_node(v[r]);
                 s.ch_rs[x] = v[r].y;
-                s.ch_dp[x] = v[r].z | (j << kParShift);
+                s.ch_dp[x] = rec_deg(v[r]) | (j << kParShift);
                 atomicAdd(&s.cc[j], 1u);
                 atomicMin(&s.cs[j], x);
             }
@@ -290,31 +348,43 @@ struct Solo {
             const uint32_t x = s.so_idx[i];
             const uint32_t pos = P + i;
             if (PB_CHECK(M.res, pos < M.n, 603)) {
-                __stcg(reinterpret_cast<uint4*>(M.rec) + pos,
-                       make_uint4(s.ch_c[x], s.ch_rs[x], s.ch_dp[x] & kDegMask, 0u));
+                __stcg(q + pos, solo_rec(s.ch_c[x], s.ch_dp[x] & kDegMask, s.ch_rs[x]));
+                // its row, read when it is a parent (soon, on small levels)
+                prefetch_row(e2, s.ch_rs[x], s.ch_dp[x] & kDegMask);
                 if (write_perm)
                     M.perm[reverse ? M.n - 1 - pos : pos] = s.ch_c[x];
             }
             mark(s.ch_c[x]);
         }
+        // the table slots and parent counters this chunk used, clear again
+        // (their last readers are behind the barriers above)
+#pragma unroll
+        for (int r = 0; r < MAXEPT; ++r)
+            if (cand[r])
+                s.tab[slot[r]] = kSoloEmpty;
+        for (uint32_t j = t; j < m; j += B) {
+            s.cs[j] = kSoloEmpty;
+            s.cc[j] = 0;
+        }
         return Q;
     }
 };
 
-// The per-edge neighbour records of a matrix (e2[k] = (c, rp[c], rp[c+1] -
-// rp[c], 0) for c = ci[k]) by one group, coalesced; columns out of range are
-// left to the CSR check.
+// The per-edge neighbour records of a matrix (e2[k] = solo_rec(c, rp[c+1] -
+// rp[c], rp[c]) for c = ci[k]) by one group, coalesced.  A column out of
+// range gets an empty record (the CSR check reports it); a valence of 4,096
+// or more does not fit a record, but such a matrix never reaches the solo
+// engine (its rows exceed every chunk).
 template <int B>
-__device__ void solo_build_edges(const MatrixView& M, uint4* e2)
+__device__ void solo_build_edges(const MatrixView& M, uint2* e2)
 {
 #pragma unroll 4
     for (uint32_t k = gtid<B>(); k < M.nnz; k += B) {
         const uint32_t c = ld_ro(M.ci + k);
-        uint4 r = make_uint4(c, 0u, 0u, 0u);
+        uint2 r = make_uint2(kSoloEmpty, 0u);
         if (c < M.n) {
             const uint32_t a = ld_ro(M.rp + c), b = ld_ro(M.rp + c + 1);
-            r.y = a;
-            r.z = b - a;
+            r = solo_rec(c, b - a, a);
         }
         __stcg(e2 + k, r);
     }
@@ -333,10 +403,16 @@ __device__ void solo_pass(Solo<B, EMAX>& so, uint32_t start, bool sorted, bool w
     uint32_t* vis = so.gvis ? so.gvis : s.vis;
     for (uint32_t i = t; i < words; i += B)
         vis[i] = 0u;
+    // the dedup table and the parent counters start clear (each chunk
+    // leaves them so)
+    for (uint32_t i = t; i < (uint32_t)SoloSmem<B, EMAX>::H; i += B)
+        s.tab[i] = kSoloEmpty;
+    s.cs[t] = kSoloEmpty;
+    s.cc[t] = 0;
     gsync<B>();
     if (t == 0) {
         const uint32_t a = ld_ro(M.rp + start), b = ld_ro(M.rp + start + 1);
-        __stcg(reinterpret_cast<uint4*>(M.rec), make_uint4(start, a, b - a, 0u));
+        __stcg(so.q, solo_rec(start, b - a, a));
         if (write_perm)
             M.perm[reverse ? M.n - 1 : 0] = start;
         so.mark(start);
@@ -390,14 +466,14 @@ __device__ void solo_pass(Solo<B, EMAX>& so, uint32_t start, bool sorted, bool w
 // gvis: ceil(n / 32) words for the visited bitmap when n > kSoloMaxN (else
 // nullptr: the bitmap is in shared memory).
 template <int B, int EMAX>
-__device__ void solo_reorder(SoloSmem<B, EMAX>& s, const MatrixView& M, const uint4* e2, uint32_t* inv,
+__device__ void solo_reorder(SoloSmem<B, EMAX>& s, const MatrixView& M, const uint2* e2, uint32_t* inv,
                              uint32_t* gvis, const Options& opt)
 {
     const uint32_t t = gtid<B>();
     const uint32_t n = M.n;
     if (t == 0)
         M.res->t_begin = globaltimer();
-    Solo<B, EMAX> so{s, M, e2, gvis};
+    Solo<B, EMAX> so{s, M, e2, reinterpret_cast<uint2*>(M.rec), gvis};
     uint32_t start = opt.start;
     if (start != kUnvisited && start >= n) {
         if (t == 0)
@@ -435,7 +511,7 @@ __device__ void solo_reorder(SoloSmem<B, EMAX>& s, const MatrixView& M, const ui
             continue;
         }
         if (t == 0)
-            s.bcast[0] = next_peripheral_start(M, opt.outnodes, last_start);
+            s.bcast[0] = so.next_start(opt.outnodes, last_start);
         gsync<B>();
         start = s.bcast[0];
         gsync<B>();
@@ -464,7 +540,7 @@ __device__ void solo_reorder(SoloSmem<B, EMAX>& s, const MatrixView& M, const ui
     }
     if (opt.want_bw) {
         for (uint32_t pos = t; pos < n; pos += B)
-            inv[__ldcg(&M.rec[pos].node)] = pos;
+            inv[rec_node(__ldcg(so.q + pos))] = pos;
         gsync<B>();
         unsigned long long bw = 0, bw0 = 0, plo = 0, phi = 0;
         for (uint32_t i = t; i < n; i += B) {

@@ -53,6 +53,7 @@ pbrcm_tuning from_context(const Context& C)
     pbrcm_tuning t;
     std::memset(&t, 0, sizeof(t));
     t.batch_pool = (uint32_t)C.batch_pool;
+    t.batch_kernel = C.batch_solo_kernel ? 1u : 0u;
     t.cluster_size = (uint32_t)std::max(1, C.cluster_size);
     t.cluster_max = (uint32_t)std::max(0, C.cluster_max);
     t.cluster_nnz = (uint32_t)std::min<uint64_t>(C.cluster_nnz, 0xFFFFFFFFu);
@@ -65,15 +66,14 @@ pbrcm_tuning from_context(const Context& C)
 
 bool valid(const pbrcm_tuning& t)
 {
-    // the batch kernels' pool shapes 0..3 and 5 (4 is the session's
-    // one-request CTA)
-    return (t.batch_pool <= 3 || t.batch_pool == 5 || t.batch_pool == 6) && t.cluster_size >= 1 && t.cluster_size <= 16 && t.cluster_nnz >= 1 &&
-           t.session_cutoff_n >= 1 && (t.session_pool == 0 || (t.session_pool >= 4 && t.session_pool < (uint32_t)kNumPools));
+    return batch_pool_ok((int)t.batch_pool) && t.batch_kernel <= 1 && t.cluster_size >= 1 && t.cluster_size <= 16 && t.cluster_nnz >= 1 &&
+           t.session_cutoff_n >= 1 && session_pool_ok((int)t.session_pool);
 }
 
 void to_context(Context& C, const pbrcm_tuning& t)
 {
     C.batch_pool = (int)t.batch_pool;
+    C.batch_solo_kernel = t.batch_kernel != 0;
     C.cluster_size = (int)t.cluster_size;
     C.cluster_max = (int)t.cluster_max;
     C.cluster_nnz = t.cluster_nnz;
@@ -90,10 +90,10 @@ bool write_file(const char* path, const pbrcm_tuning& t)
     if (!f)
         return false;
     std::fprintf(f,
-                 "%s\nversion=%s\nsms=%u\nbatch_pool=%u\ncluster_size=%u\ncluster_max=%u\ncluster_nnz=%u\n"
+                 "%s\nversion=%s\nsms=%u\nbatch_pool=%u\nbatch_kernel=%u\ncluster_size=%u\ncluster_max=%u\ncluster_nnz=%u\n"
                  "session_cutoff_n=%u\nsession_pool=%u\ntrials=%u\ndefault_ms=%.4f\nbest_ms=%.4f\n"
                  "session_default_ms=%.4f\nsession_best_ms=%.4f\n",
-                 kTuningMagic, kVersion, t.sms, t.batch_pool, t.cluster_size, t.cluster_max, t.cluster_nnz,
+                 kTuningMagic, kVersion, t.sms, t.batch_pool, t.batch_kernel, t.cluster_size, t.cluster_max, t.cluster_nnz,
                  t.session_cutoff_n, t.session_pool, t.trials, t.default_ms, t.best_ms, t.session_default_ms,
                  t.session_best_ms);
     return std::fclose(f) == 0;
@@ -145,6 +145,8 @@ bool pbrcm::load_tuning_file(const char* path, int sms, pbrcm_tuning* out)
             t.sms = (uint32_t)u;
         else if (k == "batch_pool")
             t.batch_pool = (uint32_t)u;
+        else if (k == "batch_kernel")
+            t.batch_kernel = (uint32_t)u;
         else if (k == "cluster_size")
             t.cluster_size = (uint32_t)u;
         else if (k == "cluster_max")
@@ -290,12 +292,22 @@ int32_t pbrcm_autotune(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t co
             best = t;
         }
     };
-    // 1. thread-group shape
-    for (uint32_t p : {0u, 1u, 2u, 3u, 5u, 6u}) {
-        pbrcm_tuning t = best;
-        if (p != t.batch_pool) {
-            t.batch_pool = p;
-            try_setting(t);
+    // 1. thread-group shape, with the general and (where the shape has
+    // one) the solo batch kernel
+    {
+        const pbrcm_tuning base = best;
+        for (uint32_t p = 0; p < (uint32_t)kNumPools; ++p) {
+            if (!batch_pool_ok((int)p))
+                continue;
+            for (uint32_t k = 0; k < 2; ++k) {
+                if (k == 1 && solo_max_ctas((int)p, C.sms) <= 0)
+                    continue;
+                pbrcm_tuning t = best;
+                t.batch_pool = p;
+                t.batch_kernel = k;
+                if (p != base.batch_pool || k != base.batch_kernel)
+                    try_setting(t);
+            }
         }
     }
     // 2. cluster teams for the biggest matrices: size x count

@@ -97,6 +97,9 @@ constexpr uint64_t kMaxNnz = 0xFFFFFFF0ull;
 // The one-group engine of the batch kernels (solo.cuh) keeps a matrix's
 // visited set in shared memory: matrices of at most this many nodes.
 constexpr uint32_t kSoloMaxN = 1u << 18;
+// Its 8-byte edge and queue records hold a node in 20 bits and a valence in
+// 12: matrices of at most this many nodes (and rows of at most 4,095).
+constexpr uint32_t kSoloMaxNodes = 1u << 20;
 
 // Bytes of the per-launch team words of a cooperative launch of `ctas` CTAs:
 // 2 x u64 per CTA for the level all-gather, then one u32 barrier flag per
@@ -126,7 +129,7 @@ struct BatchJob {
     unsigned long long* words;    // team > 1: zeroed team_words_bytes(team)
     const uint32_t* ready;        // nonzero once the matrix's CSR is in device memory (written by a
                                   // host-to-device copy after the CSR's copies); nullptr: already there
-    uint4* e2;                    // nnz edge records for the one-group engine (solo.cuh), or nullptr
+    uint2* e2;                    // nnz edge records for the one-group engine (solo.cuh), or nullptr
     uint32_t* inv;                // n words (the solo engine's inverse permutation)
     uint32_t* gvis;               // ceil(n / 32) words: the solo engine's visited bitmap when n > kSoloMaxN
 };

@@ -88,11 +88,14 @@ def test_mixed_batch_subset_host_overlapped(pbrcm, gpu_ctx, c4_subset):
 
 
 def test_mixed_batch_pool_shapes_identical(pbrcm, c4_subset, monkeypatch):
-    """Every pool shape (groups per CTA) gives the same permutations."""
+    """Every pool shape (groups per CTA), with the general batch kernel and
+    with the solo batch kernel, gives the oracle's permutations."""
     mats, refs = c4_subset
     small = mats[::4]
-    for pool in (0, 1, 2, 3, 5, 6):
+    shapes = [(p, k) for p in (0, 1, 2, 3, 5, 6, 7) for k in ("0", "1")]
+    for pool, solo_kernel in shapes:
         monkeypatch.setenv("PBRCM_BATCH_POOL", str(pool))
+        monkeypatch.setenv("PBRCM_BATCH_SOLO_KERNEL", solo_kernel)
         ctx = pbrcm.Context(0)
         try:
             perms, results = pbrcm.reorder_batch(small, reverse=True, ctx=ctx)

@@ -41,7 +41,8 @@ def test_autotune_keeps_permutations(pbrcm, tmp_path):
         try:
             pbrcm.tuning_load(ctx2, path)
             t2 = pbrcm.tuning_get(ctx2)
-            for k in ("batch_pool", "cluster_size", "cluster_max", "cluster_nnz", "session_cutoff_n", "session_pool"):
+            for k in ("batch_pool", "batch_kernel", "cluster_size", "cluster_max", "cluster_nnz", "session_cutoff_n",
+                      "session_pool"):
                 assert t2[k] == t[k], k
             assert t2["source"] == 1
             text = open(path).read().replace(f"sms={t['sms']}", f"sms={t['sms'] + 1}")
@@ -65,7 +66,11 @@ def test_tuning_file_read_at_context_creation(pbrcm, tmp_path, monkeypatch):
         t = pbrcm.tuning_get(ctx)
         assert (t["batch_pool"], t["cluster_size"], t["cluster_max"]) == (2, 4, 8)
         with pytest.raises(pbrcm.PbrcmError):
-            pbrcm.tuning_set(ctx, batch_pool=7)
+            pbrcm.tuning_set(ctx, batch_pool=4)  # the session's one-request shape
+        with pytest.raises(pbrcm.PbrcmError):
+            pbrcm.tuning_set(ctx, batch_pool=8)
+        with pytest.raises(pbrcm.PbrcmError):
+            pbrcm.tuning_set(ctx, batch_kernel=2)
         sms = t["sms"]
     finally:
         ctx.close()
