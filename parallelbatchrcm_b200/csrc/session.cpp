@@ -16,12 +16,15 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -82,6 +85,92 @@ private:
     std::multimap<size_t, void*> free_;
 };
 
+// Host threads for the submit-time copy of a CSR into pinned staging: one
+// thread copies pageable memory at a few GB/s, so a request of millions of
+// entries would spend milliseconds in submit and a burst of them would
+// throttle the whole stream.  run(parts, f) runs f(0) .. f(parts - 1) on the
+// pool's threads and the caller and returns when all are done; concurrent
+// callers take turns.
+class CopyPool {
+public:
+    explicit CopyPool(int threads)
+    {
+        for (int i = 0; i < threads; ++i)
+            th_.emplace_back([this] { loop(); });
+    }
+    ~CopyPool()
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (std::thread& t : th_)
+            t.join();
+    }
+    int threads() const { return (int)th_.size(); }
+    void run(int parts, const std::function<void(int)>& f)
+    {
+        std::lock_guard<std::mutex> turn(run_mu_);
+        auto job = std::make_shared<Job>();
+        job->f = &f;
+        job->parts = parts;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            job_ = job;
+            ++gen_;
+        }
+        cv_.notify_all();
+        work(*job);
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_done_.wait(lk, [&] { return job->done == job->parts; });
+        job_.reset();
+    }
+
+private:
+    struct Job {
+        const std::function<void(int)>* f = nullptr;
+        int parts = 0;
+        std::atomic<int> next{0};
+        int done = 0;  // under mu_
+    };
+    void work(Job& job)
+    {
+        // f stays valid while a part is left: run() returns only after the
+        // last part is done
+        while (true) {
+            const int p = job.next.fetch_add(1);
+            if (p >= job.parts)
+                return;
+            (*job.f)(p);
+            std::lock_guard<std::mutex> lk(mu_);
+            if (++job.done == job.parts)
+                cv_done_.notify_all();
+        }
+    }
+    void loop()
+    {
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> lk(mu_);
+        while (true) {
+            cv_.wait(lk, [&] { return stop_ || (gen_ != seen && job_); });
+            if (stop_)
+                return;
+            seen = gen_;
+            std::shared_ptr<Job> job = job_;
+            lk.unlock();
+            work(*job);
+            lk.lock();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_, run_mu_;
+    std::condition_variable cv_, cv_done_;
+    std::shared_ptr<Job> job_;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
+
 struct Request {
     uint64_t ticket = 0;
     uint32_t n = 0;
@@ -105,14 +194,17 @@ struct Request {
     int ctas = 1;       // CTAs of its launch (team size, or 1)
     int units = 1;      // share of the GPU it holds (see pbrcm_session::units_per_sm)
     int stream = 0;
-    cudaEvent_t ev = nullptr;
-    int state = 0;  // 0 queued, 1 running, 2 done
+    cudaEvent_t ev = nullptr;     // the result is back in the staging
+    cudaEvent_t ev_in = nullptr;  // the CSR is in device memory
+    bool copied = false;          // ev_in seen complete (the worker's own flag)
+    int state = 0;  // 0 queued, 1 copying in or running, 2 done
+    bool launched = false;
     int32_t rc = PBRCM_OK;
     // once done: the result and permutation, moved out of the pinned staging
     // (which goes back to the pool at once, for the next submissions)
     DevResult res_done{};
     std::vector<uint32_t> perm_done;
-    Clock::time_point t_submit, t_done;
+    Clock::time_point t_submit, t_copy, t_launch, t_done;
 };
 
 }  // namespace
@@ -140,11 +232,14 @@ struct pbrcm_session {
     uint64_t team_nnz = 1ull << 19;
     uint32_t light_team_n = 1u << 14;  // under light load, requests above this many nodes get a team
     bool big_solo = false;  // under load, big requests run as one solo CTA too (PBRCM_SESSION_BIG_SOLO)
+    bool solo_kernel = false;  // one-CTA solo requests launch the solo batch kernel
 
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Request*> queued;
-    std::vector<Request*> running;
+    std::vector<Request*> copying;  // device memory held, CSR on its way in (arrival order)
+    std::vector<Request*> running;  // kernel launched
+    size_t admitting = 0;  // being started by the worker (in no list)
     std::unordered_map<uint64_t, Request*> all;
     uint64_t next_ticket = 1;
     uint64_t bytes_in_flight = 0, peak_bytes = 0;
@@ -153,13 +248,21 @@ struct pbrcm_session {
     Clock::time_point t_first{}, t_last{};
     bool have_first = false;
     std::shared_ptr<PinnedPool> pinned_pool = std::make_shared<PinnedPool>();  // the context's (see PinnedPool)
+    std::unique_ptr<CopyPool> copy_pool;  // submit-time staging copies (PBRCM_SESSION_COPY_THREADS, 0: none)
     std::vector<cudaEvent_t> free_events;  // events of retired requests, for reuse
     std::atomic<bool> stop{false};
     std::thread worker;
+    // PBRCM_SESSION_TRACE=<path>: one CSV line per request (written when the
+    // session is destroyed): size, how it ran, and its host-clock times
+    std::string trace_path;
+    std::vector<std::string> trace;
     cudaMemPool_t pool = nullptr;
 
     void run();
+    bool start_copy(Request* r);
     bool launch(Request* r);
+    void fail(Request* r);
+    void collect(Request* r);
     void retire(Request* r);
     void decide_mode(Request* r) const;
     int choose_ctas(const Request* r) const;
@@ -205,12 +308,61 @@ size_t device_bytes(uint32_t n, uint64_t nnz, bool hub, bool solo, int team_ctas
 
 }  // namespace
 
+// Copies a CSR into its staging (rp_out, ci_out) and returns its longest
+// row; requests of 4 MB or more are cut into slices of about 1 MB (rows of
+// row_ptr with their valences, entries of col_idx) for the copy threads.
+static uint32_t copy_csr(pbrcm_session* s, const uint32_t* row_ptr, const uint32_t* col_idx, uint32_t n, uint64_t nnz,
+                  uint32_t* rp_out, uint32_t* ci_out)
+{
+    const size_t bytes = 4 * ((size_t)n + 1 + nnz);
+    const int parts = s->copy_pool && bytes >= ((size_t)4 << 20)
+                          ? (int)std::min<size_t>((size_t)s->copy_pool->threads() + 1, bytes >> 20)
+                          : 1;
+    std::vector<uint32_t> md((size_t)parts, 0u);
+    auto slice = [&](int p) {
+        const uint64_t a = (uint64_t)n * p / parts, b = (uint64_t)n * (p + 1) / parts;
+        uint32_t m = 0;
+        for (uint64_t i = a; i < b; ++i)
+            m = std::max(m, row_ptr[i + 1] - row_ptr[i]);
+        md[(size_t)p] = m;
+        std::memcpy(rp_out + a, row_ptr + a, 4 * (size_t)(b - a + (p == parts - 1 ? 1 : 0)));
+        const uint64_t c = nnz * p / parts, d = nnz * (p + 1) / parts;
+        if (d > c)
+            std::memcpy(ci_out + c, col_idx + c, 4 * (size_t)(d - c));
+    };
+    if (parts == 1)
+        slice(0);
+    else
+        s->copy_pool->run(parts, slice);
+    return *std::max_element(md.begin(), md.end());
+}
+
+// Stage 1 of a request (admitted by device memory): its device block and
+// the CSR's copy in, on its own stream; ev_in marks the copy done.  It holds
+// no CTAs yet, so that copies queued behind the copy engines never keep SMs
+// idle.
+bool pbrcm_session::start_copy(Request* r)
+{
+    cudaStream_t st = streams[r->stream];
+    if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->dev), r->dev_bytes, pool, st) != cudaSuccess)
+        return false;
+    unsigned char* D = r->dev;
+    bool ok = cudaMemcpyAsync(D + r->d_rp, r->host + r->off_rp, 4 * ((size_t)r->n + 1), cudaMemcpyHostToDevice,
+                              st) == cudaSuccess;
+    if (r->nnz)
+        ok = ok && cudaMemcpyAsync(D + r->d_ci, r->host + r->off_ci, 4 * (size_t)r->nnz, cudaMemcpyHostToDevice,
+                                   st) == cudaSuccess;
+    ok = ok && cudaEventRecord(r->ev_in, st) == cudaSuccess;
+    return ok;
+}
+
+// Stage 2 (admitted by CTAs once its CSR is in): the kernel in the mode
+// decide_mode chose, then the permutation and result back to the staging;
+// ev marks them there.
 bool pbrcm_session::launch(Request* r)
 {
     cudaStream_t st = streams[r->stream];
     Context& c = *C;
-    if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->dev), r->dev_bytes, pool, st) != cudaSuccess)
-        return false;
     unsigned char* D = r->dev;
     MatrixView M{};
     M.rp = reinterpret_cast<const uint32_t*>(D + r->d_rp);
@@ -238,12 +390,7 @@ bool pbrcm_session::launch(Request* r)
     BatchJob* d_job = reinterpret_cast<BatchJob*>(D + r->d_cnt + 16);
     BatchSlot* d_slot = reinterpret_cast<BatchSlot*>(D + r->d_cnt + 16 + sizeof(BatchJob));
     uint32_t* d_counter = reinterpret_cast<uint32_t*>(D + r->d_cnt);
-    bool ok = cudaMemcpyAsync(D + r->d_rp, r->host + r->off_rp, 4 * ((size_t)r->n + 1), cudaMemcpyHostToDevice,
-                              st) == cudaSuccess;
-    if (r->nnz)
-        ok = ok && cudaMemcpyAsync(D + r->d_ci, r->host + r->off_ci, 4 * (size_t)r->nnz, cudaMemcpyHostToDevice,
-                                   st) == cudaSuccess;
-    ok = ok && cudaMemsetAsync(D + r->d_res, 0, sizeof(DevResult), st) == cudaSuccess;
+    bool ok = cudaMemsetAsync(D + r->d_res, 0, sizeof(DevResult), st) == cudaSuccess;
     ok = ok && cudaMemsetAsync(D + r->d_gs, 0, sizeof(GridSync), st) == cudaSuccess;
     if (r->team)
         ok = ok && cudaMemsetAsync(D + r->d_agg, 0, team_words_bytes(r->ctas), st) == cudaSuccess;
@@ -265,6 +412,8 @@ bool pbrcm_session::launch(Request* r)
     } else if (r->team)
         ok = ok && launch_team(c.team_variant, M, r->opt, reinterpret_cast<GridSync*>(D + r->d_gs),
                                reinterpret_cast<unsigned long long*>(D + r->d_agg), r->ctas, st) == cudaSuccess;
+    else if (r->solo && solo_kernel)
+        ok = ok && launch_solo(small_pool, d_job, d_slot, 1, d_counter, r->opt, 1, st) == cudaSuccess;
     else
         ok = ok && launch_batch(small_pool, d_job, d_slot, 1, d_counter, r->opt, 1, false, st) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(r->host + r->off_perm, M.perm, 4 * (size_t)r->n, cudaMemcpyDeviceToHost, st) ==
@@ -276,26 +425,61 @@ bool pbrcm_session::launch(Request* r)
     return ok;
 }
 
-void pbrcm_session::retire(Request* r)
+// A request whose copy or launch could not be issued: done with
+// PBRCM_ERR_CUDA, its share released (under the session lock).
+void pbrcm_session::fail(Request* r)
 {
+    r->rc = PBRCM_ERR_CUDA;
+    r->state = 2;
+    r->t_done = Clock::now();
+    bytes_in_flight -= r->dev_bytes;
+    ctas_in_use -= r->units;
+    r->units = 0;
+    stream_busy[r->stream] -= 1;
+    ++completed;
+}
+
+// A finished request's result and permutation out of its pinned staging
+// (the worker calls this without the session lock: nothing else touches a
+// running request's staging).
+void pbrcm_session::collect(Request* r)
+{
+    r->t_done = Clock::now();
     DevResult& res = r->res_done;
     std::memcpy(&res, r->host + r->off_res, sizeof(res));
     r->rc = map_status(res.status);
     if (r->rc == PBRCM_OK)
         r->perm_done.assign(reinterpret_cast<const uint32_t*>(r->host + r->off_perm),
                             reinterpret_cast<const uint32_t*>(r->host + r->off_perm) + r->n);
+}
+
+// Bookkeeping of a collected request (under the session lock): staging and
+// event back to their pools, the GPU share it held released.
+void pbrcm_session::retire(Request* r)
+{
+    const DevResult& res = r->res_done;
     pinned_pool->put(r->host, r->host_cap);
     r->host = nullptr;
     free_events.push_back(r->ev);
+    free_events.push_back(r->ev_in);
     r->ev = nullptr;
+    r->ev_in = nullptr;
     r->state = 2;
-    r->t_done = Clock::now();
+    if (!trace_path.empty()) {
+        auto ms = [&](Clock::time_point t) { return std::chrono::duration<double, std::milli>(t - t_first).count(); };
+        char line[256];
+        std::snprintf(line, sizeof(line), "%u,%llu,%s,%d,%.3f,%.3f,%.3f,%.3f,%.3f", r->n, (unsigned long long)r->nnz,
+                      r->cluster ? "cluster" : r->team ? "team" : r->solo ? "solo" : "cta", r->ctas, ms(r->t_submit),
+                      ms(r->t_copy), ms(r->t_launch), ms(r->t_done),
+                      res.t_end > res.t_begin ? (double)(res.t_end - res.t_begin) * 1e-6 : -1.0);
+        trace.emplace_back(line);
+    }
     bytes_in_flight -= r->dev_bytes;
     ctas_in_use -= r->units;
     stream_busy[r->stream] -= 1;
     ++completed;
     lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
-    t_last = r->t_done;
+    t_last = std::max(t_last, r->t_done);
 }
 
 // How a request runs, decided when it is admitted.  A request above the
@@ -337,32 +521,44 @@ int pbrcm_session::choose_ctas(const Request* r) const
     return std::max(1, std::min(t, max_ctas));
 }
 
+// The worker, in two stages per request: a queued request is admitted by
+// device memory (start_copy: its CSR goes in on its own stream), then, once
+// the copy is done, by CTAs (launch: decide_mode picks how it runs).  It
+// retires finished requests.  The CUDA calls (event queries, copies and
+// launches) and the result copies run without the session lock, so that
+// submit() and poll() from other threads never wait behind them.
 void pbrcm_session::run()
 {
     cudaSetDevice(C->device);
+    std::vector<Request*> snap_run, snap_copy, fin, to_copy, to_launch;
     std::unique_lock<std::mutex> lk(mu);
     while (!stop.load()) {
-        bool progress = false;
-        for (size_t i = 0; i < running.size();) {
-            Request* r = running[i];
-            if (cudaEventQuery(r->ev) == cudaSuccess) {
-                retire(r);
-                running[i] = running.back();
-                running.pop_back();
-                progress = true;
-            } else {
-                ++i;
+        snap_run.assign(running.begin(), running.end());
+        snap_copy.assign(copying.begin(), copying.end());
+        lk.unlock();
+        fin.clear();
+        for (Request* r : snap_run)
+            if (cudaEventQuery(r->ev) == cudaSuccess)
+                fin.push_back(r);
+        bool newly_copied = false;
+        for (Request* r : snap_copy)
+            if (!r->copied && cudaEventQuery(r->ev_in) == cudaSuccess) {
+                r->copied = true;
+                newly_copied = true;
             }
+        for (Request* r : fin)
+            collect(r);
+        lk.lock();
+        for (Request* r : fin) {
+            retire(r);
+            running.erase(std::find(running.begin(), running.end(), r));
         }
-        // admit in arrival order while memory, CTAs and a free stream allow
-        while (!queued.empty() && running.size() < max_inflight) {
+        // stage 1, by device memory, in arrival order
+        to_copy.clear();
+        while (!queued.empty() && copying.size() + running.size() + to_copy.size() < max_inflight) {
             Request* r = queued.front();
-            if (bytes_in_flight + r->dev_bytes > cap_bytes && !running.empty())
-                break;
-            decide_mode(r);
-            const int need = choose_ctas(r);
-            const int units = r->team && !r->cluster ? need * units_per_sm : need;
-            if (ctas_in_use + units > cap_ctas && !running.empty())
+            const bool idle = running.empty() && copying.empty() && to_copy.empty();
+            if (bytes_in_flight + r->dev_bytes > cap_bytes && !idle)
                 break;
             int free_stream = -1;
             for (size_t k = 0; k < stream_busy.size(); ++k)
@@ -374,29 +570,61 @@ void pbrcm_session::run()
                 break;
             queued.pop_front();
             r->stream = free_stream;
-            r->ctas = need;
-            r->units = units;
+            r->units = 0;
             stream_busy[free_stream] += 1;
-            ctas_in_use += units;
             bytes_in_flight += r->dev_bytes;
             peak_bytes = std::max(peak_bytes, bytes_in_flight);
             r->state = 1;
-            if (!launch(r)) {
-                r->rc = PBRCM_ERR_CUDA;
-                r->state = 2;
-                r->t_done = Clock::now();
-                bytes_in_flight -= r->dev_bytes;
-                ctas_in_use -= units;
-                stream_busy[free_stream] -= 1;
-                ++completed;
-            } else {
-                running.push_back(r);
-            }
-            progress = true;
+            to_copy.push_back(r);
         }
+        // stage 2, by CTAs: the copied requests in arrival order, until one
+        // does not fit
+        to_launch.clear();
+        for (Request* r : copying) {
+            if (!r->copied)
+                continue;
+            decide_mode(r);
+            const int need = choose_ctas(r);
+            const int units = r->team && !r->cluster ? need * units_per_sm : need;
+            if (ctas_in_use + units > cap_ctas && !(running.empty() && to_launch.empty()))
+                break;
+            r->ctas = need;
+            r->units = units;
+            ctas_in_use += units;
+            to_launch.push_back(r);
+        }
+        for (Request* r : to_launch)
+            copying.erase(std::find(copying.begin(), copying.end(), r));
+        if (!to_copy.empty() || !to_launch.empty()) {
+            admitting = to_copy.size() + to_launch.size();
+            lk.unlock();
+            for (Request* r : to_copy) {
+                r->t_copy = Clock::now();
+                r->launched = start_copy(r);
+            }
+            for (Request* r : to_launch) {
+                r->t_launch = Clock::now();
+                r->launched = launch(r);
+            }
+            lk.lock();
+            admitting = 0;
+            for (Request* r : to_copy) {
+                if (r->launched)
+                    copying.push_back(r);
+                else
+                    fail(r);
+            }
+            for (Request* r : to_launch) {
+                if (r->launched)
+                    running.push_back(r);
+                else
+                    fail(r);
+            }
+        }
+        const bool progress = !fin.empty() || !to_copy.empty() || !to_launch.empty() || newly_copied;
         if (progress)
             cv_done.notify_all();
-        if (running.empty() && queued.empty())
+        if (running.empty() && copying.empty() && queued.empty())
             cv_work.wait(lk, [&] { return stop.load() || !queued.empty(); });
         else if (!progress) {
             lk.unlock();
@@ -439,7 +667,11 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
     s->small_pool = s->C->session_pool;
     s->team_cutoff_n = s->C->session_cutoff_n;
     s->max_ctas = std::max(1, team_max_ctas(s->C->team_variant, s->C->sms));
-    s->cap_ctas = std::max(1, batch_max_ctas(s->small_pool, s->C->sms));
+    // one-CTA requests on the solo batch kernel where the shape has one (it
+    // may fit more CTAs on an SM than the general kernel)
+    const int solo_cap = s->C->solo && s->C->batch_solo_kernel ? solo_max_ctas(s->small_pool, s->C->sms) : 0;
+    s->solo_kernel = solo_cap > 0;
+    s->cap_ctas = std::max(1, s->solo_kernel ? solo_cap : batch_max_ctas(s->small_pool, s->C->sms));
     s->units_per_sm = std::max(1, s->cap_ctas / std::max(1, s->C->sms));
     s->stream_busy.assign(s->streams.size(), 0);
     if (const char* e = std::getenv("PBRCM_SESSION_TEAM_NNZ"))
@@ -454,6 +686,16 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
         s->big_solo = std::atoi(e) != 0;
     if (const char* e = std::getenv("PBRCM_SESSION_LIGHT_TEAM_N"))
         s->light_team_n = (uint32_t)std::max(1L, std::atol(e));
+    {
+        const unsigned hc = std::thread::hardware_concurrency();
+        int ct = (int)std::min(8u, std::max(1u, hc / 2)) - 1;  // the submitting thread copies too
+        if (const char* e = std::getenv("PBRCM_SESSION_COPY_THREADS"))
+            ct = std::max(0, std::min(64, std::atoi(e)));
+        if (ct > 0)
+            s->copy_pool.reset(new (std::nothrow) CopyPool(ct));
+    }
+    if (const char* e = std::getenv("PBRCM_SESSION_TRACE"))
+        s->trace_path = e;
     if (const char* e = std::getenv("PBRCM_SESSION_CLUSTER_MAX"))
         s->cluster_max = std::max(0, std::min(16, std::atoi(e)));
     if (cudaDeviceGetDefaultMemPool(&s->pool, s->C->device) != cudaSuccess) {
@@ -484,12 +726,22 @@ void pbrcm_session_destroy(pbrcm_session* s)
         Request* r = kv.second;
         if (r->ev)
             cudaEventDestroy(r->ev);
+        if (r->ev_in)
+            cudaEventDestroy(r->ev_in);
         if (r->host)
             s->pinned_pool->put(r->host, r->host_cap);
         delete r;
     }
     for (cudaEvent_t e : s->free_events)
         cudaEventDestroy(e);
+    if (!s->trace_path.empty()) {
+        if (FILE* f = std::fopen(s->trace_path.c_str(), "w")) {
+            std::fprintf(f, "n,nnz,mode,ctas,submit_ms,copy_ms,launch_ms,done_ms,device_ms\n");
+            for (const std::string& l : s->trace)
+                std::fprintf(f, "%s\n", l.c_str());
+            std::fclose(f);
+        }
+    }
     for (cudaStream_t st : s->streams) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
@@ -510,10 +762,44 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     r->opt = make_options(opts, kModeFull);
     apply_team_shape(*s->C, r->opt);
     r->opt.phantom = 0;
-    uint32_t maxdeg = 0;
-    for (uint32_t i = 0; i < n; ++i)
-        maxdeg = std::max(maxdeg, row_ptr[i + 1] - row_ptr[i]);
-    r->maxdeg = maxdeg;
+    // pinned staging: [rp | ci | view | perm_out | result]
+    size_t o = 0;
+    r->off_rp = o;
+    o = align16(o + 4 * ((size_t)n + 1));
+    r->off_ci = o;
+    o = align16(o + 4 * (size_t)nnz);
+    r->off_view = o;
+    o = align16(o + sizeof(BatchJob) + sizeof(BatchSlot));
+    r->off_perm = o;
+    o = align16(o + 4 * (size_t)n);
+    r->off_res = o;
+    o = align16(o + sizeof(DevResult));
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        cudaSetDevice(s->C->device);
+        r->host = static_cast<unsigned char*>(s->pinned_pool->get(o, r->host_cap));
+        for (cudaEvent_t* e : {&r->ev, &r->ev_in}) {
+            if (!s->free_events.empty()) {
+                *e = s->free_events.back();
+                s->free_events.pop_back();
+            } else if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) {
+                *e = nullptr;
+            }
+        }
+        if (!r->host || !r->ev || !r->ev_in) {
+            s->pinned_pool->put(r->host, r->host_cap);
+            for (cudaEvent_t e : {r->ev, r->ev_in})
+                if (e)
+                    s->free_events.push_back(e);
+            delete r;
+            return PBRCM_ERR_OOM;
+        }
+    }
+    // the CSR into the staging and its longest row, in slices on the copy
+    // threads when it is large
+    r->maxdeg = copy_csr(s, row_ptr, col_idx, n, nnz, reinterpret_cast<uint32_t*>(r->host + r->off_rp),
+                         reinterpret_cast<uint32_t*>(r->host + r->off_ci));
+    const uint32_t maxdeg = r->maxdeg;
     const int emax_small = kPools[s->small_pool].gemax;
     r->big = n > s->team_cutoff_n || maxdeg > (uint32_t)emax_small;
     r->solo_able = s->C->solo && nnz > 0 && maxdeg <= (uint32_t)emax_small && n <= kSoloMaxNodes;
@@ -534,40 +820,15 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     r->d_hub = offs[9];
     r->d_e2 = offs[10];
     r->d_gvis = offs[11];
-    if (r->dev_bytes > s->cap_bytes) {
-        delete r;
-        return PBRCM_ERR_BUSY;
-    }
-    size_t o = 0;
-    r->off_rp = o;
-    o = align16(o + 4 * ((size_t)n + 1));
-    r->off_ci = o;
-    o = align16(o + 4 * (size_t)nnz);
-    r->off_view = o;
-    o = align16(o + sizeof(BatchJob) + sizeof(BatchSlot));
-    r->off_perm = o;
-    o = align16(o + 4 * (size_t)n);
-    r->off_res = o;
-    o = align16(o + sizeof(DevResult));
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        cudaSetDevice(s->C->device);
-        r->host = static_cast<unsigned char*>(s->pinned_pool->get(o, r->host_cap));
-        if (!s->free_events.empty()) {
-            r->ev = s->free_events.back();
-            s->free_events.pop_back();
-        }
-        if (!r->host || (!r->ev && cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess)) {
+        if (r->dev_bytes > s->cap_bytes) {
             s->pinned_pool->put(r->host, r->host_cap);
+            s->free_events.push_back(r->ev);
+            s->free_events.push_back(r->ev_in);
             delete r;
-            return PBRCM_ERR_OOM;
+            return PBRCM_ERR_BUSY;
         }
-    }
-    std::memcpy(r->host + r->off_rp, row_ptr, 4 * ((size_t)n + 1));
-    if (nnz)
-        std::memcpy(r->host + r->off_ci, col_idx, 4 * (size_t)nnz);
-    {
-        std::lock_guard<std::mutex> lk(s->mu);
         r->ticket = s->next_ticket++;
         r->t_submit = Clock::now();
         if (!s->have_first) {
@@ -618,7 +879,9 @@ int32_t pbrcm_session_drain(pbrcm_session* s)
     if (!s)
         return PBRCM_ERR_ARG;
     std::unique_lock<std::mutex> lk(s->mu);
-    s->cv_done.wait(lk, [&] { return s->queued.empty() && s->running.empty(); });
+    s->cv_done.wait(lk, [&] {
+        return s->queued.empty() && s->copying.empty() && s->running.empty() && s->admitting == 0;
+    });
     return PBRCM_OK;
 }
 
