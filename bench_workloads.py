@@ -478,7 +478,7 @@ def run_mixed(args, ws, rank, local, extras: bool = True):
 
     count = int(os.environ.get("PBRCM_BENCH_COUNT", "4096"))
     serve_n = int(os.environ.get("PBRCM_BENCH_SERVE", "160")) if ws == 1 and extras else 0
-    rates = [float(x) for x in os.environ.get("PBRCM_BENCH_RATES", "100,100000").split(",")]
+    rates = [float(x) for x in os.environ.get("PBRCM_BENCH_RATES", "400,100000").split(",")]
     t0 = time.time()
     specs = mixed_specs(count, ws, rank)
     mats = generate(specs)

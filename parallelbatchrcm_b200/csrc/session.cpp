@@ -44,45 +44,86 @@ using Clock = std::chrono::steady_clock;
 
 inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-// Pinned host memory, recycled by size class (powers of two).  One pool per
-// context, shared by its sessions (a session that starts finds the staging
-// earlier ones left behind); its own lock.
+// Pinned host memory for the sessions' staging: slabs from cudaHostAlloc,
+// carved first-fit into blocks that coalesce again when freed.  One pool per
+// context, shared by its sessions (a session finds the staging earlier ones
+// left behind); its own lock.  Pinning costs milliseconds per call, so the
+// pool grows in slabs of at least its current size and never shrinks: a
+// burst of requests that fit before fits again.
 class PinnedPool {
 public:
     ~PinnedPool()
     {
-        for (auto& kv : free_)
-            cudaFreeHost(kv.second);
+        for (const Slab& sl : slabs_)
+            cudaFreeHost(sl.base);
     }
     void* get(size_t bytes, size_t& cap)
     {
         std::lock_guard<std::mutex> lk(mu_);
-        size_t c = 4096;
-        while (c < bytes)
-            c <<= 1;
-        auto it = free_.find(c);
-        if (it != free_.end()) {
-            void* p = it->second;
+        bytes = (std::max<size_t>(bytes, 1) + 4095) & ~(size_t)4095;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second.size < bytes)
+                continue;
+            unsigned char* p = it->first;
+            const Block b = it->second;
             free_.erase(it);
-            cap = c;
+            if (b.size > bytes)
+                free_.emplace(p + bytes, Block{b.size - bytes, b.slab});
+            cap = bytes;
             return p;
         }
-        void* p = nullptr;
-        if (cudaHostAlloc(&p, c, cudaHostAllocDefault) != cudaSuccess)
+        const size_t sz = std::max(bytes, std::max(total_, (size_t)64 << 20));
+        void* raw = nullptr;
+        if (cudaHostAlloc(&raw, sz, cudaHostAllocDefault) != cudaSuccess)
             return nullptr;
-        cap = c;
-        return p;
+        auto* base = static_cast<unsigned char*>(raw);
+        slabs_.push_back(Slab{base, sz});
+        total_ += sz;
+        if (sz > bytes)
+            free_.emplace(base + bytes, Block{sz - bytes, slabs_.size() - 1});
+        cap = bytes;
+        return base;
     }
-    void put(void* p, size_t cap)
+    void put(void* ptr, size_t cap)
     {
+        if (!ptr)
+            return;
         std::lock_guard<std::mutex> lk(mu_);
-        if (p)
-            free_.emplace(cap, p);
+        auto* p = static_cast<unsigned char*>(ptr);
+        size_t slab = 0;
+        while (slab < slabs_.size() && !(p >= slabs_[slab].base && p < slabs_[slab].base + slabs_[slab].size))
+            ++slab;
+        Block b{cap, slab};
+        // coalesce with the blocks on either side (same slab only)
+        auto next = free_.lower_bound(p);
+        if (next != free_.end() && next->first == p + b.size && next->second.slab == slab) {
+            b.size += next->second.size;
+            next = free_.erase(next);
+        }
+        if (next != free_.begin()) {
+            auto prev = std::prev(next);
+            if (prev->first + prev->second.size == p && prev->second.slab == slab) {
+                prev->second.size += b.size;
+                return;
+            }
+        }
+        free_.emplace(p, b);
     }
+    size_t pinned_bytes() const { return total_; }
 
 private:
+    struct Slab {
+        unsigned char* base;
+        size_t size;
+    };
+    struct Block {
+        size_t size;
+        size_t slab;
+    };
     std::mutex mu_;
-    std::multimap<size_t, void*> free_;
+    std::vector<Slab> slabs_;
+    std::map<unsigned char*, Block> free_;  // free blocks by address
+    size_t total_ = 0;
 };
 
 // Host threads for the submit-time copy of a CSR into pinned staging: one
@@ -205,6 +246,9 @@ struct Request {
     DevResult res_done{};
     std::vector<uint32_t> perm_done;
     Clock::time_point t_submit, t_copy, t_launch, t_done;
+    float stage_ms = 0.f;  // host time of the submit-time staging copy
+    float get_ms = 0.f;    // ... of taking the staging and events
+    float lock_ms = 0.f;
 };
 
 }  // namespace
@@ -468,10 +512,12 @@ void pbrcm_session::retire(Request* r)
     if (!trace_path.empty()) {
         auto ms = [&](Clock::time_point t) { return std::chrono::duration<double, std::milli>(t - t_first).count(); };
         char line[256];
-        std::snprintf(line, sizeof(line), "%u,%llu,%s,%d,%.3f,%.3f,%.3f,%.3f,%.3f", r->n, (unsigned long long)r->nnz,
+        std::snprintf(line, sizeof(line), "%u,%llu,%s,%d,%.3f,%.3f,%.3f,%.3f,%.3f,%.3f,%.3f,%.3f,%d", r->n,
+                      (unsigned long long)r->nnz,
                       r->cluster ? "cluster" : r->team ? "team" : r->solo ? "solo" : "cta", r->ctas, ms(r->t_submit),
                       ms(r->t_copy), ms(r->t_launch), ms(r->t_done),
-                      res.t_end > res.t_begin ? (double)(res.t_end - res.t_begin) * 1e-6 : -1.0);
+                      res.t_end > res.t_begin ? (double)(res.t_end - res.t_begin) * 1e-6 : -1.0, (double)r->stage_ms,
+                      (double)r->get_ms, (double)r->lock_ms, (int)0);
         trace.emplace_back(line);
     }
     bytes_in_flight -= r->dev_bytes;
@@ -736,7 +782,7 @@ void pbrcm_session_destroy(pbrcm_session* s)
         cudaEventDestroy(e);
     if (!s->trace_path.empty()) {
         if (FILE* f = std::fopen(s->trace_path.c_str(), "w")) {
-            std::fprintf(f, "n,nnz,mode,ctas,submit_ms,copy_ms,launch_ms,done_ms,device_ms\n");
+            std::fprintf(f, "n,nnz,mode,ctas,submit_ms,copy_ms,launch_ms,done_ms,device_ms,stage_ms,get_ms,lock_ms,miss\n");
             for (const std::string& l : s->trace)
                 std::fprintf(f, "%s\n", l.c_str());
             std::fclose(f);
@@ -774,8 +820,10 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     o = align16(o + 4 * (size_t)n);
     r->off_res = o;
     o = align16(o + sizeof(DevResult));
+    const Clock::time_point t_get = Clock::now();
     {
         std::lock_guard<std::mutex> lk(s->mu);
+        r->lock_ms = (float)std::chrono::duration<double, std::milli>(Clock::now() - t_get).count();
         cudaSetDevice(s->C->device);
         r->host = static_cast<unsigned char*>(s->pinned_pool->get(o, r->host_cap));
         for (cudaEvent_t* e : {&r->ev, &r->ev_in}) {
@@ -797,8 +845,11 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     }
     // the CSR into the staging and its longest row, in slices on the copy
     // threads when it is large
+    const Clock::time_point t_stage = Clock::now();
+    r->get_ms = (float)std::chrono::duration<double, std::milli>(t_stage - t_get).count();
     r->maxdeg = copy_csr(s, row_ptr, col_idx, n, nnz, reinterpret_cast<uint32_t*>(r->host + r->off_rp),
                          reinterpret_cast<uint32_t*>(r->host + r->off_ci));
+    r->stage_ms = (float)std::chrono::duration<double, std::milli>(Clock::now() - t_stage).count();
     const uint32_t maxdeg = r->maxdeg;
     const int emax_small = kPools[s->small_pool].gemax;
     r->big = n > s->team_cutoff_n || maxdeg > (uint32_t)emax_small;
