@@ -349,8 +349,6 @@ struct Solo {
             const uint32_t pos = P + i;
             if (PB_CHECK(M.res, pos < M.n, 603)) {
                 __stcg(q + pos, solo_rec(s.ch_c[x], s.ch_dp[x] & kDegMask, s.ch_rs[x]));
-                // its row, read when it is a parent (soon, on small levels)
-                prefetch_row(e2, s.ch_rs[x], s.ch_dp[x] & kDegMask);
                 if (write_perm)
                     M.perm[reverse ? M.n - 1 - pos : pos] = s.ch_c[x];
             }
