@@ -1873,6 +1873,32 @@ __device__ void validate_group(const MatrixView& M, uint32_t* red)
     gsync<B>();
 }
 
+// validate_group without the column pass: row pointers and the largest
+// valence (the solo batch kernel tests the columns while it builds the edge
+// records, solo_build_edges).
+template <int B>
+__device__ void validate_rows(const MatrixView& M, uint32_t* red)
+{
+    const uint32_t t = gtid<B>();
+    uint32_t mx = 0;
+    bool bad = false;
+    for (uint32_t i = t; i < M.n; i += B) {
+        const uint32_t a = ld_ro(M.rp + i), b = ld_ro(M.rp + i + 1);
+        if (b < a || b > M.nnz)
+            bad = true;
+        else
+            mx = max(mx, b - a);
+    }
+    if (t == 0 && (ld_ro(M.rp) != 0 || ld_ro(M.rp + M.n) != M.nnz))
+        bad = true;
+    if (bad)
+        set_status(M.res, kErrArg, 200);
+    mx = block_reduce_max<B, uint32_t>(mx, red);
+    if (t == 0)
+        atomicMax(&M.res->maxdeg, mx);
+    gsync<B>();
+}
+
 // Bounded wait of a thread group for a matrix's CSR to arrive (the word
 // `ready` is written by a host-to-device copy after the CSR's copies).  A
 // wait that runs out posts PBRCM_ERR_TIMEOUT for the matrix.  The word is

@@ -153,7 +153,7 @@ __device__ void group_take_solo(unsigned char* raw, const BatchJob* jobs, const 
             if (!arrived)
                 continue;
         }
-        validate_group<GB>(job.M, s.tmp32);
+        validate_rows<GB>(job.M, s.tmp32);
         if (read_status(job.M.res) != 0)
             continue;
         // rows longer than a chunk, or no room for edge records (the host
@@ -165,8 +165,10 @@ __device__ void group_take_solo(unsigned char* raw, const BatchJob* jobs, const 
                 set_status(job.M.res, kNeedHub, 0);
             continue;
         }
-        solo_build_edges<GB>(job.M, job.e2);
+        solo_build_edges<GB>(job.M, job.e2);  // tests the columns too
         gsync<GB>();
+        if (read_status(job.M.res) != 0)
+            continue;
         solo_reorder<GB, GE>(s, job.M, job.e2, job.inv, job.M.n > kSoloMaxN ? job.gvis : nullptr, opt);
         gsync<GB>();
     }

@@ -376,16 +376,22 @@ struct Solo {
 template <int B>
 __device__ void solo_build_edges(const MatrixView& M, uint2* e2)
 {
-#pragma unroll 4
+    bool bad = false;
+#pragma unroll 8
     for (uint32_t k = gtid<B>(); k < M.nnz; k += B) {
         const uint32_t c = ld_ro(M.ci + k);
         uint2 r = make_uint2(kSoloEmpty, 0u);
         if (c < M.n) {
             const uint32_t a = ld_ro(M.rp + c), b = ld_ro(M.rp + c + 1);
             r = solo_rec(c, b - a, a);
+        } else {
+            bad = true;
         }
         __stcg(e2 + k, r);
     }
+    // the CSR check's column test (validate_rows leaves it to this pass)
+    if (bad)
+        set_status(M.res, kErrArg, 200);
 }
 
 // One ordered BFS pass from `start` by one solo group.  Fills rec[0 ..
@@ -537,8 +543,17 @@ __device__ void solo_reorder(SoloSmem<B, EMAX>& s, const MatrixView& M, const ui
         return;
     }
     if (opt.want_bw) {
-        for (uint32_t pos = t; pos < n; pos += B)
-            inv[rec_node(__ldcg(so.q + pos))] = pos;
+        // the inverse permutation (four records in flight per thread)
+        for (uint32_t pos = t; pos < n; pos += 4 * B) {
+            uint2 r[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                r[u] = pos + u * B < n ? __ldcg(so.q + pos + u * B) : make_uint2(0u, 0u);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (pos + u * B < n)
+                    inv[rec_node(r[u])] = pos + u * B;
+        }
         gsync<B>();
         unsigned long long bw = 0, bw0 = 0, plo = 0, phi = 0;
         for (uint32_t i = t; i < n; i += B) {
@@ -546,11 +561,24 @@ __device__ void solo_reorder(SoloSmem<B, EMAX>& s, const MatrixView& M, const ui
             if (a == e)
                 continue;
             const uint32_t me = __ldcg(inv + i);
-            uint32_t mnr = kUnvisited, mxr = 0;
-            for (uint32_t k = a; k < e; ++k) {
-                const uint32_t p = __ldcg(inv + ld_ro(M.ci + k));
-                mnr = min(mnr, p);
-                mxr = max(mxr, p);
+            uint32_t mnr = kUnvisited, mxr = 0, c0 = 0, c1 = 0;
+            // the row's columns four at a time, then their positions (the
+            // loads of a group side by side)
+            for (uint32_t k = a; k < e; k += 4) {
+                uint32_t c[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    c[u] = k + u < e ? ld_ro(M.ci + k + u) : kUnvisited;
+                if (k == a)
+                    c0 = c[0];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (c[u] != kUnvisited) {
+                        const uint32_t p = __ldcg(inv + c[u]);
+                        mnr = min(mnr, p);
+                        mxr = max(mxr, p);
+                        c1 = c[u];
+                    }
             }
             // computeBandwidth (main.cpp:143-184): max(row - min, max - row)
             const unsigned long long b1 = me >= mnr ? (unsigned long long)(me - mnr) : 0ull;
@@ -559,7 +587,6 @@ __device__ void solo_reorder(SoloSmem<B, EMAX>& s, const MatrixView& M, const ui
             plo += b1;
             phi += b2;
             // initial bandwidth: first / last stored column (main.cpp:114-129)
-            const uint32_t c0 = ld_ro(M.ci + a), c1 = ld_ro(M.ci + e - 1);
             const unsigned long long i0 = i >= c0 ? i - c0 : 0, i1 = c1 >= i ? c1 - i : 0;
             bw0 = max(bw0, max(i0, i1));
         }
