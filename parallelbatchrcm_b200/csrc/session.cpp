@@ -267,13 +267,13 @@ struct pbrcm_session {
     int units_per_sm = 1;
     int cap_ctas = 0;              // units the running requests may hold together
     int ctas_in_use = 0;           // units held
-    int team_min = 4, team_max = 64;
+    int team_min = 2, team_max = 64;
     int idle_team = 0;             // team of a large request that finds the GPU idle (0 = no boost)
     // largest cluster team (0: cooperative teams only).  Off by default: on
     // the Poisson serving mix, cooperative teams of up to 64 CTAs served
     // 289 reorders/s against 202-229 for clusters of <= 4-16 CTAs
     int cluster_max = 0;
-    uint64_t team_nnz = 1ull << 19;
+    uint64_t team_nnz = 1ull << 20;  // entries per team CTA (measured on the Poisson mix: 2^20 and a minimum of 2 CTAs served 630-692 reorders/s all at once against 630-661 for 2^19 and 4, 551 for 2^21)
     uint32_t light_team_n = 1u << 14;  // under light load, requests above this many nodes get a team
     bool big_solo = false;  // under load, big requests run as one solo CTA too (PBRCM_SESSION_BIG_SOLO)
     bool solo_kernel = false;  // one-CTA solo requests launch the solo batch kernel
