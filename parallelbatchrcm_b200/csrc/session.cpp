@@ -273,7 +273,10 @@ struct pbrcm_session {
     // the Poisson serving mix, cooperative teams of up to 64 CTAs served
     // 289 reorders/s against 202-229 for clusters of <= 4-16 CTAs
     int cluster_max = 0;
-    uint64_t team_nnz = 1ull << 20;  // entries per team CTA (measured on the Poisson mix: 2^20 and a minimum of 2 CTAs served 630-692 reorders/s all at once against 630-661 for 2^19 and 4, 551 for 2^21)
+    // entries per team CTA (measured on the Poisson mix all at once: 2^20
+    // with teams of at least 2 CTAs served 630-692 reorders/s, 2^19 with at
+    // least 4 served 630-661, 2^21 served 551)
+    uint64_t team_nnz = 1ull << 20;
     uint32_t light_team_n = 1u << 14;  // under light load, requests above this many nodes get a team
     bool big_solo = false;  // under load, big requests run as one solo CTA too (PBRCM_SESSION_BIG_SOLO)
     bool solo_kernel = false;  // one-CTA solo requests launch the solo batch kernel
