@@ -402,6 +402,14 @@ int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
         }
         break;
     }
+    // every hand-over sequence ends within the four attempts (hub, then wide
+    // or team, then hub again); an internal code still standing means the
+    // hand-over logic went round in a circle: a check failure of its own
+    // (where 900 + the code's offset), not a CSR check's
+    if (out->status == kNeedHub || out->status == kNeedWide || out->status == kNeedTeam) {
+        out->where = 900u + (out->status - (uint32_t)kNeedHub);
+        out->status = kErrCheck;
+    }
     return PBRCM_OK;
 }
 

@@ -66,6 +66,27 @@ def test_noalloc_equals_allocating_entry_point(pbrcm, gpu_ctx):
     assert rc == 0 and np.array_equal(got.cpu().numpy().astype(np.uint32), g["perm"])
 
 
+def test_noalloc_at_its_node_limit(pbrcm, gpu_ctx):
+    """n = 2^20 exactly (a 1024 x 1024 grid): the node table and the queue
+    records fill the static scratch; same permutation and result as the
+    allocating entry point."""
+    import torch
+    from parallelbatchrcm_b200 import _lib, gen
+    L = _lib.lib()
+    m = gen.grid2d(1024, 1024, seed=29)
+    assert m.n == 1 << 20
+    rp, ci = _device((m.row_ptr, m.col_idx))
+    stream = torch.cuda.current_stream().cuda_stream
+    want, ref = pbrcm.reorder_device(rp, ci, reverse=True, ctx=gpu_ctx)
+    got = torch.full((m.n,), -1, dtype=torch.int32, device="cuda")
+    rc, res = _noalloc(L, rp, ci, got, True, stream)
+    assert rc == 0 and res["status"] == 0
+    assert torch.equal(got, want)
+    for k in ("start_node", "peripheral_passes", "eccentricity", "levels", "placed", "bandwidth", "profile"):
+        assert res[k] == ref[k], k
+    assert res["device_ms"] > 0
+
+
 def test_noalloc_refuses_inputs_beyond_its_limits(pbrcm, gpu_ctx):
     import torch
     from parallelbatchrcm_b200 import _lib
