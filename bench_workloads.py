@@ -548,7 +548,7 @@ def run_mixed(args, ws, rank, local, extras: bool = True):
     abytes = sum(reorder_bytes(int(rp.shape[0] - 1), int(ci.shape[0]), r["peripheral_passes"])
                  for (rp, ci), r in zip(mats, res))
     achieved = abytes / (statistics.mean(times) / 1e3) / 1e9
-    traffic = profile_value("k_reorder_batch_mixed_batch_4096.md", "traffic_bytes_per_launch")
+    traffic = profile_value("k_solo_batch_mixed_batch_4096.md", "traffic_bytes_per_launch")
 
     serve = None
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=dev)
@@ -601,7 +601,7 @@ def run_mixed(args, ws, rank, local, extras: bool = True):
                 "d2h_bytes_per_step": int(4 * sum_n + 64 * count), "steps": e2e_steps,
                 "what": "pbrcm_reorder_batch: pinned host CSRs in, permutations to pinned host buffers"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "kernel": "k_reorder_batch (the batch launch)",
+                     "peak_kind": peak_kind, "kernel": "k_solo_batch (the batch launch)",
                      "algorithmic_bytes_per_launch": abytes, "traffic": traffic},
         "serve": serve,
         "grid3d_128": g3_out,
