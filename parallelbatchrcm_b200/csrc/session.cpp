@@ -269,10 +269,13 @@ struct pbrcm_session {
     int ctas_in_use = 0;           // units held
     int team_min = 2, team_max = 64;
     int idle_team = 0;             // team of a large request that finds the GPU idle (0 = no boost)
-    // largest cluster team (0: cooperative teams only).  Off by default: on
-    // the Poisson serving mix, cooperative teams of up to 64 CTAs served
-    // 289 reorders/s against 202-229 for clusters of <= 4-16 CTAs
-    int cluster_max = 0;
+    // largest cluster team (0: cooperative teams only).  A big request whose
+    // rows fit a CTA's chunk runs as one thread-block cluster of up to this
+    // many CTAs (hardware cluster barrier, all-gather in distributed shared
+    // memory; a plain launch beside the others): on the Poisson mix all at
+    // once, 884 / 840 reorders/s with clusters of up to 16 / 8 CTAs against
+    // 726 with cooperative teams only
+    int cluster_max = 16;
     // entries per team CTA (measured on the Poisson mix all at once: 2^20
     // with teams of at least 2 CTAs served 630-692 reorders/s, 2^19 with at
     // least 4 served 630-661, 2^21 served 551)
