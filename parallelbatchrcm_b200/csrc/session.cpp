@@ -247,8 +247,7 @@ struct Request {
     std::vector<uint32_t> perm_done;
     Clock::time_point t_submit, t_copy, t_launch, t_done;
     float stage_ms = 0.f;  // host time of the submit-time staging copy
-    float get_ms = 0.f;    // ... of taking the staging and events
-    float lock_ms = 0.f;
+    float get_ms = 0.f;    // ... of taking the staging and events (the session lock included)
 };
 
 }  // namespace
@@ -518,12 +517,12 @@ void pbrcm_session::retire(Request* r)
     if (!trace_path.empty()) {
         auto ms = [&](Clock::time_point t) { return std::chrono::duration<double, std::milli>(t - t_first).count(); };
         char line[256];
-        std::snprintf(line, sizeof(line), "%u,%llu,%s,%d,%.3f,%.3f,%.3f,%.3f,%.3f,%.3f,%.3f,%.3f,%d", r->n,
+        std::snprintf(line, sizeof(line), "%u,%llu,%s,%d,%.3f,%.3f,%.3f,%.3f,%.3f,%.3f,%.3f", r->n,
                       (unsigned long long)r->nnz,
                       r->cluster ? "cluster" : r->team ? "team" : r->solo ? "solo" : "cta", r->ctas, ms(r->t_submit),
                       ms(r->t_copy), ms(r->t_launch), ms(r->t_done),
                       res.t_end > res.t_begin ? (double)(res.t_end - res.t_begin) * 1e-6 : -1.0, (double)r->stage_ms,
-                      (double)r->get_ms, (double)r->lock_ms, (int)0);
+                      (double)r->get_ms);
         trace.emplace_back(line);
     }
     bytes_in_flight -= r->dev_bytes;
@@ -789,7 +788,7 @@ void pbrcm_session_destroy(pbrcm_session* s)
         cudaEventDestroy(e);
     if (!s->trace_path.empty()) {
         if (FILE* f = std::fopen(s->trace_path.c_str(), "w")) {
-            std::fprintf(f, "n,nnz,mode,ctas,submit_ms,copy_ms,launch_ms,done_ms,device_ms,stage_ms,get_ms,lock_ms,miss\n");
+            std::fprintf(f, "n,nnz,mode,ctas,submit_ms,copy_ms,launch_ms,done_ms,device_ms,stage_ms,get_ms\n");
             for (const std::string& l : s->trace)
                 std::fprintf(f, "%s\n", l.c_str());
             std::fclose(f);
@@ -830,7 +829,6 @@ int32_t pbrcm_session_submit(pbrcm_session* s, const uint32_t* row_ptr, const ui
     const Clock::time_point t_get = Clock::now();
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        r->lock_ms = (float)std::chrono::duration<double, std::milli>(Clock::now() - t_get).count();
         cudaSetDevice(s->C->device);
         r->host = static_cast<unsigned char*>(s->pinned_pool->get(o, r->host_cap));
         for (cudaEvent_t* e : {&r->ev, &r->ev_in}) {
