@@ -734,6 +734,7 @@ struct Smem {
     unsigned long long tmp64[2 * W + 2];
     unsigned long long gat64[2 * W + 2];  // all-gather reduction (its own buffer)
     uint32_t scanbuf[5][W];               // one per block_scan1 call site
+    uint32_t wq[EMAX / B][W];             // collect: child edges per (round, warp)
     uint32_t hist[256];
     // chunk scalars
     uint32_t m, Ec, Q, Qdeg, hub, npre;
@@ -857,31 +858,28 @@ struct Chunk {
     // computes the edge offsets of the ranked children.
     __device__ Agg collect(bool sorted, bool from_pre = false)
     {
-        const uint32_t t = gtid<B>();
+        const uint32_t t = gtid<B>(), lane = t & 31u, w = t >> 5;
         const uint32_t m = s.m, Ec = s.Ec;
-        const uint32_t ept = (Ec + B - 1) / B;
-        const uint32_t e0 = t * ept;
-        const uint32_t e1 = min(e0 + ept, Ec);
-        uint32_t j = 0;
-        if (e0 < e1) {
-            uint32_t lo = 0, hi = m;  // soff[lo] <= e0 < soff[hi]
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (s.soff[mid] <= e0)
-                    lo = mid;
-                else
-                    hi = mid;
-            }
-            j = lo;
-        }
+        // thread t takes the edges e = t + B r: a warp loads consecutive
+        // entries of the parents' rows (coalesced), and edge order is
+        // (round r, warp, lane), the order the compaction below keeps
         uint32_t c[MAXEPT], jj[MAXEPT], key[MAXEPT], kk[MAXEPT];
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
-            const uint32_t e = e0 + r;
+            const uint32_t e = t + (uint32_t)B * r;
             c[r] = kUnvisited;
-            if (e < e1) {
-                while (s.soff[j + 1] <= e)
-                    ++j;
+            jj[r] = 0;
+            kk[r] = 1;
+            if (e < Ec) {
+                // the edge's parent: the last j < m with soff[j] <= e (a
+                // parent of valence 0 owns no edge)
+                uint32_t j = 0;
+#pragma unroll
+                for (uint32_t d = (uint32_t)B / 2u; d > 0; d >>= 1) {
+                    const uint32_t mid = j + d;
+                    if (mid < m && s.soff[mid] <= e)
+                        j = mid;
+                }
                 const uint32_t k = e - s.soff[j];
                 const uint32_t idx = s.prs[j] + k;
                 jj[r] = j;
@@ -900,31 +898,45 @@ struct Chunk {
             if (c[r] != kUnvisited && PB_CHECK(M.res, c[r] < M.n, 103))
                 nd[r] = ld_node(M.node + c[r]);
         }
-        uint32_t nvalid = 0;
+        // the child edges (claimed by this edge's key) compacted in edge
+        // order: a ballot per warp and round, then the (round, warp) counts
+        uint32_t pos[MAXEPT];
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
-            if (c[r] != kUnvisited && c[r] < M.n && claim_of(M, nd[r]) == key[r])
-                ++nvalid;
-            else
+            if (!(c[r] != kUnvisited && c[r] < M.n && claim_of(M, nd[r]) == key[r]))
                 c[r] = kUnvisited;
+            const uint32_t bal = __ballot_sync(kFull, c[r] != kUnvisited);
+            pos[r] = __popc(bal & ((1u << lane) - 1u));
+            if (lane == 0)
+                s.wq[r][w] = __popc(bal);
         }
-        uint32_t Q;
-        uint32_t q = block_scan1<B>(nvalid, Q, s.scanbuf[1]);
+        gsync<B>();
+        uint32_t Q = 0;
 #pragma unroll
         for (int r = 0; r < MAXEPT; ++r) {
-            const uint32_t e = e0 + r;
-            if (e < e1) {
+#pragma unroll
+            for (int i = 0; i < Smem<B, EMAX>::W; ++i) {
+                const uint32_t n_ = s.wq[r][i];
+                pos[r] += (uint32_t)i < w ? n_ : 0u;
+                Q += n_;
+            }
+            // the rounds before this one
+            if (r + 1 < MAXEPT)
+                pos[r + 1] += Q;
+        }
+#pragma unroll
+        for (int r = 0; r < MAXEPT; ++r) {
+            const uint32_t e = t + (uint32_t)B * r;
+            if (e < Ec) {
+                const uint32_t q = pos[r];
                 if (kk[r] == 0)
                     s.cs[jj[r]] = q;
-                if (c[r] != kUnvisited) {
-                    if (PB_CHECK(M.res, q < (uint32_t)EMAX, 104)) {
-                        s.ch_node[q] = c[r];
-                        s.ch_rs[q] = nd[r].y;
-                        s.ch_deg[q] = nd[r].z;
-                        s.ch_par[q] = jj[r];
-                        atomicAdd(&s.cc[jj[r]], 1u);
-                    }
-                    ++q;
+                if (c[r] != kUnvisited && PB_CHECK(M.res, q < (uint32_t)EMAX, 104)) {
+                    s.ch_node[q] = c[r];
+                    s.ch_rs[q] = nd[r].y;
+                    s.ch_deg[q] = nd[r].z;
+                    s.ch_par[q] = jj[r];
+                    atomicAdd(&s.cc[jj[r]], 1u);
                 }
             }
         }
