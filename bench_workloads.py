@@ -452,6 +452,14 @@ def measure_grid3d(P, ctx, m, args, ws, stream, flush, dev, cpu: bool):
         "result": {"start": res["start_node"], "passes": res["peripheral_passes"], "ecc": res["eccentricity"],
                    "levels": res["levels"], "bandwidth": res["bandwidth"], "profile": res["profile"]},
     }
+    # the latency view: the reorder is a chain of dependent BFS levels (each
+    # search pass and the final pass walk about `levels` of them; the last
+    # search pass runs beside the final pass), so time per level of that chain
+    # says more than the HBM fraction
+    chain = res["peripheral_passes"] * res["levels"]
+    out["level_chain"] = {"levels": chain, "us_per_level": t_dev * 1e6 / args.steps / max(1, chain),
+                          "what": "passes x levels of the final order (the last search pass runs beside the "
+                                  "final pass); device time per level of that chain"}
     if cpu:
         try:
             threads = os.cpu_count() or 1
