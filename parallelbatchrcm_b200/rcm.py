@@ -195,6 +195,53 @@ def bandwidth(row_ptr, col_idx, perm, ctx: Context | None = None):
     return bw.value, bw0.value, prof.value
 
 
+# the pbrcm_matrix array of a batch as a numpy record view, so that a batch
+# of thousands of matrices is described by column assignments rather than
+# one ctypes field write at a time
+_MATRIX_DTYPE = np.dtype({
+    "names": [n for n, _ in Matrix._fields_],
+    "formats": [np.uint64, np.uint64, np.uint32, np.uint32, np.uint64, np.uint64],
+    "offsets": [getattr(Matrix, n).offset for n, _ in Matrix._fields_],
+    "itemsize": ctypes.sizeof(Matrix),
+})
+
+
+def _matrix_array(row_ptr, col_idx, n, nnz, perm_out):
+    """pbrcm_matrix[len(n)] from per-matrix address / size lists."""
+    arr = (Matrix * len(n))()
+    if len(n):
+        v = np.frombuffer(arr, dtype=_MATRIX_DTYPE)
+        v["row_ptr"] = row_ptr
+        v["col_idx"] = col_idx
+        v["n"] = n
+        v["nnz"] = nnz
+        v["perm_out"] = perm_out
+    return arr
+
+
+class BatchResults(Sequence):
+    """The per-matrix results of a batch: a sequence of result dicts, each
+    built when first read (a batch of thousands of matrices returns without
+    building them all)."""
+
+    def __init__(self, res):
+        self._res = res
+        self._d = [None] * len(res)
+
+    def __len__(self) -> int:
+        return len(self._d)
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[k] for k in range(*i.indices(len(self)))]
+        if i < 0:
+            i += len(self)
+        d = self._d[i]
+        if d is None:
+            d = self._d[i] = self._res[i].as_dict()
+        return d
+
+
 def reorder_batch(mats: Sequence, *, reverse: bool = True, start: int | None = None, want_bandwidth: bool = True,
                   ctx: Context | None = None, raise_on_error: bool = True, perms_out: Sequence | None = None,
                   **opt_kw):
@@ -202,9 +249,7 @@ def reorder_batch(mats: Sequence, *, reverse: bool = True, start: int | None = N
     launch.  perms_out: optional uint32 host arrays (n entries each, e.g.
     pinned) that receive the permutations.  Returns (list of perms, list of
     result dicts)."""
-    keep = []
-    arr = (Matrix * len(mats))()
-    perms = []
+    keep, perms, ns = [], [], []
     for i, m in enumerate(mats):
         rp, ci = _u32(m[0]), _u32(m[1])
         n = rp.shape[0] - 1
@@ -214,42 +259,35 @@ def reorder_batch(mats: Sequence, *, reverse: bool = True, start: int | None = N
                 raise ValueError("perms_out[i] must be a contiguous uint32 array of n entries")
         else:
             p = np.empty(max(n, 1), dtype=np.uint32)
-        keep += [rp, ci]
+        keep.append((rp, ci))
         perms.append(p)
-        arr[i].row_ptr = rp.ctypes.data
-        arr[i].col_idx = ci.ctypes.data
-        arr[i].n = n
-        arr[i].nnz = ci.shape[0]
-        arr[i].perm_out = p.ctypes.data
+        ns.append(n)
+    arr = _matrix_array([rp.ctypes.data for rp, _ in keep], [ci.ctypes.data for _, ci in keep], ns,
+                        [ci.shape[0] for _, ci in keep], [p.ctypes.data for p in perms])
     res = (Result * len(mats))()
     o = default_options(reverse=reverse, start=start, want_bandwidth=want_bandwidth, **opt_kw)
     rc = _lib.lib().pbrcm_reorder_batch(_h(ctx), arr, len(mats), ctypes.byref(o), res)
     if raise_on_error:
         _check(rc, "pbrcm_reorder_batch")
-    out = [r.as_dict() for r in res]
-    return [p[: (np.asarray(m[0]).shape[0] - 1)] for p, m in zip(perms, mats)], out
+    return [p[:n] for p, n in zip(perms, ns)], BatchResults(res)
 
 
 def reorder_batch_device(mats: Sequence, *, reverse: bool = True, ctx: Context | None = None, stream=None,
                          raise_on_error: bool = True, **opt_kw):
     """Batched reorder of device-resident (row_ptr, col_idx, perm_out) torch
-    tensors.  Returns the result dicts."""
+    tensors.  Returns the results (a sequence of result dicts)."""
     import torch
 
-    arr = (Matrix * len(mats))()
-    for i, (rp, ci, po) in enumerate(mats):
-        arr[i].row_ptr = rp.data_ptr()
-        arr[i].col_idx = ci.data_ptr()
-        arr[i].n = rp.numel() - 1
-        arr[i].nnz = ci.numel()
-        arr[i].perm_out = po.data_ptr()
+    arr = _matrix_array([m[0].data_ptr() for m in mats], [m[1].data_ptr() for m in mats],
+                        [m[0].numel() - 1 for m in mats], [m[1].numel() for m in mats],
+                        [m[2].data_ptr() for m in mats])
     res = (Result * len(mats))()
     o = default_options(reverse=reverse, **opt_kw)
     st = ctypes.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
     rc = _lib.lib().pbrcm_reorder_batch_device(_h(ctx), arr, len(mats), ctypes.byref(o), res, st)
     if raise_on_error:
         _check(rc, "pbrcm_reorder_batch_device")
-    return [r.as_dict() for r in res]
+    return BatchResults(res)
 
 
 def autotune(mats: Sequence, *, ctx: Context, cache_path: str | None = None, reverse: bool = True,
