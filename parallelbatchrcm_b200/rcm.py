@@ -206,6 +206,11 @@ _MATRIX_DTYPE = np.dtype({
 })
 
 
+def _addr(a: np.ndarray) -> int:
+    """Data address of a numpy array (cheaper than a.ctypes.data)."""
+    return a.__array_interface__["data"][0]
+
+
 def _matrix_array(row_ptr, col_idx, n, nnz, perm_out):
     """pbrcm_matrix[len(n)] from per-matrix address / size lists."""
     arr = (Matrix * len(n))()
@@ -262,8 +267,8 @@ def reorder_batch(mats: Sequence, *, reverse: bool = True, start: int | None = N
         keep.append((rp, ci))
         perms.append(p)
         ns.append(n)
-    arr = _matrix_array([rp.ctypes.data for rp, _ in keep], [ci.ctypes.data for _, ci in keep], ns,
-                        [ci.shape[0] for _, ci in keep], [p.ctypes.data for p in perms])
+    arr = _matrix_array([_addr(rp) for rp, _ in keep], [_addr(ci) for _, ci in keep], ns,
+                        [ci.shape[0] for _, ci in keep], [_addr(p) for p in perms])
     res = (Result * len(mats))()
     o = default_options(reverse=reverse, start=start, want_bandwidth=want_bandwidth, **opt_kw)
     rc = _lib.lib().pbrcm_reorder_batch(_h(ctx), arr, len(mats), ctypes.byref(o), res)
