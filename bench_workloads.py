@@ -667,7 +667,12 @@ def run_mixed_reference(args, ws, rank):
         "steps": len(timed), "warmup": args.warmup, "ms_per_step": t * 1e3 / len(timed), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded mixed 2-D / 3-D grids and random geometric graphs, shuffled labels)",
-        "config": {"workload": f"mixed_batch_{count}", "matrices_per_gpu": count, "sum_nnz": sum_nnz, "seed": 42},
+        "config": {"workload": f"mixed_batch_{count}", "matrices_per_gpu": count,
+                   "sum_n": sum(int(rp.shape[0]) - 1 for rp, _ in mats), "sum_nnz": sum_nnz,
+                   "n_range": [500, 200_000], "mix": "40% 2-D grid, 30% 3-D grid, 30% RGG k 4..12", "seed": 42,
+                   "reverse": True, "start": "auto",
+                   "l2": f"inputs larger than L2 ({4 * (sum(int(rp.shape[0]) for rp, _ in mats) + sum_nnz) / 1e9:.1f} GB of CSRs)",
+                   "parallelism": f"host threads, {count} matrices, no exchange"},
         "gnnz_per_s": value * (sum_nnz / count) / 1e9,
         "cpu_baseline": {"value": value, "unit": "reorders/s", "cores": thr, "kind": kind,
                          "sample": f"each step: the whole stream of {count} matrices, findPeripheral + "
