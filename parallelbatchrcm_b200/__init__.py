@@ -10,7 +10,7 @@ from .rcm import (  # noqa: F401
     AUTO_START, DEBUG_PHANTOM_CTA, GPU_BATCH, Context, Graph, PbrcmError, Session, SimplePeripheral, bandwidth,
     check_bandwidth, check_permutation, compute_bandwidth, connect_device, default_options, find_peripheral,
     load_hicsr, load_mtx,
-    max_valency, store_hicsr,
+    max_valency, store_hicsr, BatchResults, PreparedBatch,
     permute, permute_device, prepare_csr, reorder, reorder_batch, reorder_batch_device, reorder_device,
     reorder_device_noalloc, store_mtx, autotune, tuning_get, tuning_set, tuning_load,
 )

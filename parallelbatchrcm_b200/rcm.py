@@ -247,6 +247,46 @@ class BatchResults(Sequence):
         return d
 
 
+class PreparedBatch:
+    """A batch's matrix descriptors built once, for a caller that reorders the
+    same buffers again and again (a service that refills fixed pinned
+    staging, or device buffers, per call: the library then replays its
+    captured launch, and the binding skips rebuilding thousands of
+    descriptors).  Holds references to the buffers.
+
+    Host form: ``PreparedBatch(mats, perms_out=None)`` with (row_ptr, col_idx)
+    numpy arrays; device form: ``PreparedBatch(dmats, device=True)`` with
+    (row_ptr, col_idx, perm_out) torch tensors.  Pass it to reorder_batch /
+    reorder_batch_device in place of the list."""
+
+    def __init__(self, mats: Sequence, perms_out: Sequence | None = None, device: bool = False):
+        self.device = device
+        self.count = len(mats)
+        if device:
+            self.mats = list(mats)
+            self.ns = [m[0].numel() - 1 for m in self.mats]
+            self.arr = _matrix_array([m[0].data_ptr() for m in self.mats], [m[1].data_ptr() for m in self.mats],
+                                     self.ns, [m[1].numel() for m in self.mats],
+                                     [m[2].data_ptr() for m in self.mats])
+            return
+        keep, perms, ns = [], [], []
+        for i, m in enumerate(mats):
+            rp, ci = _u32(m[0]), _u32(m[1])
+            n = rp.shape[0] - 1
+            if perms_out is not None:
+                p = perms_out[i]
+                if p.dtype != np.uint32 or not p.flags.c_contiguous or p.shape[0] < n:
+                    raise ValueError("perms_out[i] must be a contiguous uint32 array of n entries")
+            else:
+                p = np.empty(max(n, 1), dtype=np.uint32)
+            keep.append((rp, ci))
+            perms.append(p)
+            ns.append(n)
+        self.mats, self.perms, self.ns = keep, perms, ns
+        self.arr = _matrix_array([_addr(rp) for rp, _ in keep], [_addr(ci) for _, ci in keep], ns,
+                                 [ci.shape[0] for _, ci in keep], [_addr(p) for p in perms])
+
+
 def reorder_batch(mats: Sequence, *, reverse: bool = True, start: int | None = None, want_bandwidth: bool = True,
                   ctx: Context | None = None, raise_on_error: bool = True, perms_out: Sequence | None = None,
                   **opt_kw):
@@ -254,27 +294,15 @@ def reorder_batch(mats: Sequence, *, reverse: bool = True, start: int | None = N
     launch.  perms_out: optional uint32 host arrays (n entries each, e.g.
     pinned) that receive the permutations.  Returns (list of perms, list of
     result dicts)."""
-    keep, perms, ns = [], [], []
-    for i, m in enumerate(mats):
-        rp, ci = _u32(m[0]), _u32(m[1])
-        n = rp.shape[0] - 1
-        if perms_out is not None:
-            p = perms_out[i]
-            if p.dtype != np.uint32 or not p.flags.c_contiguous or p.shape[0] < n:
-                raise ValueError("perms_out[i] must be a contiguous uint32 array of n entries")
-        else:
-            p = np.empty(max(n, 1), dtype=np.uint32)
-        keep.append((rp, ci))
-        perms.append(p)
-        ns.append(n)
-    arr = _matrix_array([_addr(rp) for rp, _ in keep], [_addr(ci) for _, ci in keep], ns,
-                        [ci.shape[0] for _, ci in keep], [_addr(p) for p in perms])
-    res = (Result * len(mats))()
+    pb = mats if isinstance(mats, PreparedBatch) else PreparedBatch(mats, perms_out)
+    if pb.device:
+        raise ValueError("a device PreparedBatch goes to reorder_batch_device")
+    res = (Result * pb.count)()
     o = default_options(reverse=reverse, start=start, want_bandwidth=want_bandwidth, **opt_kw)
-    rc = _lib.lib().pbrcm_reorder_batch(_h(ctx), arr, len(mats), ctypes.byref(o), res)
+    rc = _lib.lib().pbrcm_reorder_batch(_h(ctx), pb.arr, pb.count, ctypes.byref(o), res)
     if raise_on_error:
         _check(rc, "pbrcm_reorder_batch")
-    return [p[:n] for p, n in zip(perms, ns)], BatchResults(res)
+    return [p[:n] for p, n in zip(pb.perms, pb.ns)], BatchResults(res)
 
 
 def reorder_batch_device(mats: Sequence, *, reverse: bool = True, ctx: Context | None = None, stream=None,
@@ -283,13 +311,13 @@ def reorder_batch_device(mats: Sequence, *, reverse: bool = True, ctx: Context |
     tensors.  Returns the results (a sequence of result dicts)."""
     import torch
 
-    arr = _matrix_array([m[0].data_ptr() for m in mats], [m[1].data_ptr() for m in mats],
-                        [m[0].numel() - 1 for m in mats], [m[1].numel() for m in mats],
-                        [m[2].data_ptr() for m in mats])
-    res = (Result * len(mats))()
+    pb = mats if isinstance(mats, PreparedBatch) else PreparedBatch(mats, device=True)
+    if not pb.device:
+        raise ValueError("a host PreparedBatch goes to reorder_batch")
+    res = (Result * pb.count)()
     o = default_options(reverse=reverse, **opt_kw)
     st = ctypes.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
-    rc = _lib.lib().pbrcm_reorder_batch_device(_h(ctx), arr, len(mats), ctypes.byref(o), res, st)
+    rc = _lib.lib().pbrcm_reorder_batch_device(_h(ctx), pb.arr, pb.count, ctypes.byref(o), res, st)
     if raise_on_error:
         _check(rc, "pbrcm_reorder_batch_device")
     return BatchResults(res)

@@ -72,3 +72,24 @@ def test_status_strings(pbrcm):
     assert L.pbrcm_status_string(0) == b"ok"
     assert b"connected" in L.pbrcm_status_string(2)
     assert L.pbrcm_version().startswith(b"pbrcm-b200")
+
+
+def test_prepared_batch_descriptors():
+    """The binding's batch descriptors (pbrcm_matrix) carry each buffer's
+    address and sizes; results come back as a sequence of dicts."""
+    import numpy as np
+    from parallelbatchrcm_b200 import rcm
+    from parallelbatchrcm_b200._lib import Result
+    mats = [(np.array([0, 1, 2], dtype=np.uint32), np.array([1, 0], dtype=np.uint32)),
+            (np.array([0, 0], dtype=np.uint32), np.zeros(0, dtype=np.uint32))]
+    pb = rcm.PreparedBatch(mats)
+    assert pb.count == 2 and not pb.device
+    for i, (rp, ci) in enumerate(pb.mats):
+        d = pb.arr[i]
+        assert d.row_ptr == rp.ctypes.data and (d.col_idx or 0) == ci.ctypes.data
+        assert d.n == rp.shape[0] - 1 and d.nnz == ci.shape[0]
+        assert d.perm_out == pb.perms[i].ctypes.data
+    res = (Result * 3)()
+    res[2].status = 9
+    br = rcm.BatchResults(res)
+    assert len(br) == 3 and br[-1]["status"] == 9 and [r["status"] for r in br] == [0, 0, 9]

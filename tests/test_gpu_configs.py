@@ -120,15 +120,21 @@ def test_batch_graph_replay_between_other_batches(pbrcm, c4_subset):
         pinned = [(torch.from_numpy(rp.view(np.int32)).pin_memory().numpy().view(np.uint32),
                    torch.from_numpy(ci.view(np.int32)).pin_memory().numpy().view(np.uint32)) for rp, ci in a]
         outs = [torch.empty(rp.shape[0] - 1, dtype=torch.int32).pin_memory().numpy().view(np.uint32) for rp, _ in a]
+        dprep = pbrcm.PreparedBatch(dm, device=True)
+        hprep = pbrcm.PreparedBatch(pinned, perms_out=outs)
         for rep in range(3):
             for _, _, p in dm:
                 p.fill_(-1)
-            res = pbrcm.reorder_batch_device(dm, reverse=True, ctx=ctx)  # captured, then replayed
+            # captured, then replayed (the list, then its prepared descriptors)
+            res = pbrcm.reorder_batch_device(dm if rep == 0 else dprep, reverse=True, ctx=ctx)
             _check(a, ra, [p.cpu().numpy() for _, _, p in dm], res)
             pbrcm.reorder_batch(b, reverse=True, ctx=ctx)  # pageable: plain launches over the staging
             for o in outs:
                 o.fill(0xFFFFFFFF)
-            perms, res = pbrcm.reorder_batch(pinned, reverse=True, ctx=ctx, perms_out=outs)
+            if rep == 0:
+                perms, res = pbrcm.reorder_batch(pinned, reverse=True, ctx=ctx, perms_out=outs)
+            else:
+                perms, res = pbrcm.reorder_batch(hprep, reverse=True, ctx=ctx)
             _check(a, ra, perms, res)
             pbrcm.reorder_batch(b[: 8 + 8 * rep], reverse=True, ctx=ctx)
     finally:
