@@ -304,7 +304,7 @@ def _batched_step(P, ctx, db, stream):
     import torch
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    res = P.reorder_batch_device(dmats, reverse=True, ctx=ctx, stream=stream)
+    res = P.reorder_batch_device(db, reverse=True, ctx=ctx, stream=stream)
     e1.record(stream)
     e1.synchronize()
     return e0.elapsed_time(e1), res
