@@ -160,12 +160,28 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
     const int maxc = batch_max_ctas(v, C.sms);
     if (maxc <= 0)
         return PBRCM_ERR_CUDA;
+    // host buffers: a permutation buffer in pinned memory is written by the
+    // kernel itself (its device-side address; no copy back after the
+    // kernel), and a matrix whose col_idx follows its row_ptr in memory
+    // comes in with one copy instead of two
+    std::vector<uint32_t*> pdirect(host ? count : 0, nullptr);
+    for (uint32_t j = 0; j < count && host; ++j) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, mats[j].perm_out) == cudaSuccess && a.type == cudaMemoryTypeHost &&
+            a.devicePointer)
+            pdirect[j] = static_cast<uint32_t*>(a.devicePointer);
+        else
+            cudaGetLastError();
+    }
+    auto joined = [&](uint32_t j) {
+        return mats[j].nnz && reinterpret_cast<const char*>(mats[j].col_idx) ==
+                                  reinterpret_cast<const char*>(mats[j].row_ptr) + 4 * ((size_t)mats[j].n + 1);
+    };
     // graph capture: device buffers, or host buffers that are all pinned (a
     // copy from pageable memory cannot be captured)
     bool use_graph = C.batch_graphs;
     for (uint32_t j = 0; j < count && use_graph && host; ++j)
-        use_graph = is_pinned(mats[j].row_ptr) && (!mats[j].nnz || is_pinned(mats[j].col_idx)) &&
-                    is_pinned(mats[j].perm_out);
+        use_graph = is_pinned(mats[j].row_ptr) && (!mats[j].nnz || is_pinned(mats[j].col_idx)) && pdirect[j];
     // the wait for a wave is bounded; the bound grows with the bytes to copy
     // (at least 1 GB/s)
     size_t in_bytes = 0;
@@ -238,15 +254,21 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
             const pbrcm_matrix& m = mats[j];
             if (host) {
                 slot[j].rp = off;
-                off = align128(off + 4 * ((size_t)m.n + 1));
-                slot[j].ci = off;
-                off = align128(off + 4 * (size_t)m.nnz);
+                if (joined(j)) {  // the host layout, so that one copy brings both
+                    slot[j].ci = off + 4 * ((size_t)m.n + 1);
+                    off = align128(slot[j].ci + 4 * (size_t)m.nnz);
+                } else {
+                    off = align128(off + 4 * ((size_t)m.n + 1));
+                    slot[j].ci = off;
+                    off = align128(off + 4 * (size_t)m.nnz);
+                }
             }
             slot[j].node = off;
             off = align16(off + 16 * (size_t)m.n);
             slot[j].rec = off;
             off = align16(off + 16 * (size_t)m.n);
-            if (host) {
+            slot[j].perm = 0;
+            if (host && !pdirect[j]) {
                 slot[j].perm = off;
                 off = align16(off + 4 * (size_t)m.n);
             }
@@ -308,7 +330,7 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
             J.M.nnz = (uint32_t)m.nnz;
             J.M.node = reinterpret_cast<NodeEntry*>(A + slot[j].node);
             J.M.rec = reinterpret_cast<PosRec*>(A + slot[j].rec);
-            J.M.perm = host ? reinterpret_cast<uint32_t*>(A + slot[j].perm) : m.perm_out;
+            J.M.perm = !host ? m.perm_out : pdirect[j] ? pdirect[j] : reinterpret_cast<uint32_t*>(A + slot[j].perm);
             J.M.hub = nullptr;
             J.M.res = C.d_bres + q;
             J.team = q < nbig ? 1 : team[q];
@@ -395,10 +417,14 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
                 for (; q < count && wave[q] == w && ok; ++q) {
                     const pbrcm_matrix& m = mats[order[q]];
                     const Slot& sl = slot[order[q]];
-                    ok = cudaMemcpyAsync(A + sl.rp, m.row_ptr, 4 * ((size_t)m.n + 1), cudaMemcpyHostToDevice, cs) ==
-                             cudaSuccess &&
-                         (!m.nnz || cudaMemcpyAsync(A + sl.ci, m.col_idx, 4 * (size_t)m.nnz, cudaMemcpyHostToDevice,
-                                                    cs) == cudaSuccess);
+                    if (joined(order[q]))
+                        ok = cudaMemcpyAsync(A + sl.rp, m.row_ptr, 4 * ((size_t)m.n + 1 + m.nnz),
+                                             cudaMemcpyHostToDevice, cs) == cudaSuccess;
+                    else
+                        ok = cudaMemcpyAsync(A + sl.rp, m.row_ptr, 4 * ((size_t)m.n + 1), cudaMemcpyHostToDevice,
+                                             cs) == cudaSuccess &&
+                             (!m.nnz || cudaMemcpyAsync(A + sl.ci, m.col_idx, 4 * (size_t)m.nnz,
+                                                        cudaMemcpyHostToDevice, cs) == cudaSuccess);
                 }
                 ok = ok && cudaMemcpyAsync(C.d_ready + w, C.h_one, sizeof(uint32_t), cudaMemcpyHostToDevice, cs) ==
                                cudaSuccess;
@@ -411,11 +437,13 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
             ok = cudaEventRecord(C.ev1, st) == cudaSuccess;
         ok = ok && cudaMemcpyAsync(C.h_bres, C.d_bres, sizeof(DevResult) * count, cudaMemcpyDeviceToHost, st) ==
                        cudaSuccess;
-        // every permutation straight behind the kernel (issued while it
-        // runs); a matrix that fails leaves its perm_out unspecified
+        // every permutation not written in place straight behind the kernel
+        // (issued while it runs); a matrix that fails leaves its perm_out
+        // unspecified
         for (uint32_t q = 0; q < count && ok && host; ++q)
-            ok = cudaMemcpyAsync(mats[order[q]].perm_out, jobs[q].M.perm, 4 * (size_t)mats[order[q]].n,
-                                 cudaMemcpyDeviceToHost, st) == cudaSuccess;
+            if (!pdirect[order[q]])
+                ok = cudaMemcpyAsync(mats[order[q]].perm_out, jobs[q].M.perm, 4 * (size_t)mats[order[q]].n,
+                                     cudaMemcpyDeviceToHost, st) == cudaSuccess;
         if (use_graph) {
             cudaGraph_t g = nullptr;
             const bool ended = cudaStreamEndCapture(st, &g) == cudaSuccess;
@@ -460,8 +488,9 @@ int32_t pbrcm::run_batch(Context& C, const pbrcm_matrix* mats, uint32_t count, c
             launch_validate(M.rp, M.ci, M.n, M.nnz, M.res, C.sms, st) != cudaSuccess ||
             launch_team(C.team_variant, H, topt, C.d_gs, C.d_agg, C.team_ctas, st) != cudaSuccess ||
             cudaMemcpyAsync(&res[q], M.res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-            (host && cudaMemcpyAsync(mats[order[q]].perm_out, M.perm, 4 * (size_t)M.n, cudaMemcpyDeviceToHost, st) !=
-                         cudaSuccess) ||
+            (host && !pdirect[order[q]] &&
+             cudaMemcpyAsync(mats[order[q]].perm_out, M.perm, 4 * (size_t)M.n, cudaMemcpyDeviceToHost, st) !=
+                 cudaSuccess) ||
             cudaStreamSynchronize(st) != cudaSuccess)
             return PBRCM_ERR_CUDA;
     }

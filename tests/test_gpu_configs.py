@@ -141,6 +141,42 @@ def test_batch_graph_replay_between_other_batches(pbrcm, c4_subset):
         ctx.close()
 
 
+def test_batch_pinned_slab_in_place(pbrcm, c4_subset):
+    """Host matrices laid out in one pinned slab (row_ptr, col_idx and the
+    permutation of each matrix side by side): one copy brings a matrix's CSR
+    in, the kernel writes each permutation into the slab itself; captured on
+    the first call, replayed on the second."""
+    import torch
+    mats, refs = c4_subset
+    mats, refs = mats[::3], refs[::3]
+    words = sum(rp.shape[0] + ci.shape[0] + rp.shape[0] - 1 for rp, ci in mats)
+    slab = torch.empty(words, dtype=torch.int32).pin_memory()
+    flat = slab.numpy().view(np.uint32)
+    hm, hp, o = [], [], 0
+    for rp, ci in mats:
+        a = flat[o:o + rp.shape[0]]
+        a[:] = rp
+        o += rp.shape[0]
+        b = flat[o:o + ci.shape[0]]
+        b[:] = ci
+        o += ci.shape[0]
+        p = flat[o:o + rp.shape[0] - 1]
+        o += rp.shape[0] - 1
+        hm.append((a, b))
+        hp.append(p)
+    ctx = pbrcm.Context(0)
+    try:
+        prep = pbrcm.PreparedBatch(hm, perms_out=hp)
+        for _ in range(2):
+            for p in hp:
+                p.fill(0xFFFFFFFF)
+            perms, res = pbrcm.reorder_batch(prep, reverse=True, ctx=ctx)
+            _check(mats, refs, perms, res)
+            _check(mats, refs, hp, res)
+    finally:
+        ctx.close()
+
+
 def test_batch_large_matrices_global_visited(pbrcm, gpu_ctx, oracle_mod):
     """Matrices over 2^18 nodes in a batch: the one-group engine keeps their
     visited bitmap in global memory (the others in shared memory)."""
