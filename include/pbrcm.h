@@ -228,6 +228,9 @@ typedef struct pbrcm_tuning {
     uint32_t session_cutoff_n; /* serving: requests with more nodes run on a cooperative team */
     uint32_t session_pool;     /* serving: CTA shape of the other requests (0 = 512 threads,
                                   5 = 256 threads, three per SM, 4 = 128 threads, four per SM) */
+    uint32_t session_team_nnz; /* serving: a team request gets one CTA per this many entries */
+    uint32_t session_cluster_max; /* serving: largest thread-block-cluster team (0 = cooperative
+                                  teams only) */
     uint32_t sms;              /* streaming multiprocessors of the device it was measured on */
     uint32_t trials;           /* settings measured */
     uint32_t source;           /* 0 built-in defaults, 1 a tuning file, 2 measured or set */

@@ -72,6 +72,7 @@ class Tuning(ctypes.Structure):
         ("batch_pool", ctypes.c_uint32), ("batch_kernel", ctypes.c_uint32),
         ("cluster_size", ctypes.c_uint32), ("cluster_max", ctypes.c_uint32),
         ("cluster_nnz", ctypes.c_uint32), ("session_cutoff_n", ctypes.c_uint32), ("session_pool", ctypes.c_uint32),
+        ("session_team_nnz", ctypes.c_uint32), ("session_cluster_max", ctypes.c_uint32),
         ("sms", ctypes.c_uint32),
         ("trials", ctypes.c_uint32), ("source", ctypes.c_uint32), ("default_ms", ctypes.c_float),
         ("best_ms", ctypes.c_float), ("session_default_ms", ctypes.c_float), ("session_best_ms", ctypes.c_float),

@@ -174,6 +174,8 @@ int32_t Context::init(int dev)
     tn.cluster_nnz = 1u << 18;
     tn.session_cutoff_n = 1u << 18;
     tn.session_pool = 0;
+    tn.session_team_nnz = 1u << 20;
+    tn.session_cluster_max = 16;
     if (const char* tp = std::getenv("PBRCM_TUNING")) {
         if (load_tuning_file(tp, sms, &tn))
             tuned = 1;
@@ -185,6 +187,8 @@ int32_t Context::init(int dev)
     session_pool = env_int("PBRCM_SESSION_POOL", (int)tn.session_pool);
     if (!session_pool_ok(session_pool))
         session_pool = 0;
+    session_team_nnz = (uint32_t)std::max(1, env_int("PBRCM_SESSION_TEAM_NNZ", (int)tn.session_team_nnz));
+    session_cluster_max = std::max(0, std::min(16, env_int("PBRCM_SESSION_CLUSTER_MAX", (int)tn.session_cluster_max)));
     solo = env_int("PBRCM_SOLO", 1) != 0;
     batch_solo_kernel = env_int("PBRCM_BATCH_SOLO_KERNEL", (int)tn.batch_kernel) != 0;
     batch_graphs = env_int("PBRCM_BATCH_GRAPHS", 1) != 0;

@@ -49,6 +49,8 @@ struct Context {
     uint32_t session_cutoff_n = 1u << 18;
     int session_pool = 0;  // serving: kPools shape of the one-CTA requests (512-thread CTAs: on the
                            // Poisson mix 264 reorders/s against 219 for 256-thread CTAs)
+    uint32_t session_team_nnz = 1u << 20;  // serving: entries per team CTA
+    int session_cluster_max = 16;          // serving: largest cluster team (0: cooperative teams only)
     // where the batch / serving shape came from: 0 built-in defaults, 1 a
     // tuning file, 2 pbrcm_autotune or pbrcm_tuning_set
     uint32_t tuned = 0;

@@ -726,8 +726,8 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
     s->cap_ctas = std::max(1, s->solo_kernel ? solo_cap : batch_max_ctas(s->small_pool, s->C->sms));
     s->units_per_sm = std::max(1, s->cap_ctas / std::max(1, s->C->sms));
     s->stream_busy.assign(s->streams.size(), 0);
-    if (const char* e = std::getenv("PBRCM_SESSION_TEAM_NNZ"))
-        s->team_nnz = std::max<uint64_t>(1, std::strtoull(e, nullptr, 10));
+    s->team_nnz = std::max<uint64_t>(1, s->C->session_team_nnz);  // context: tuned, or PBRCM_SESSION_TEAM_NNZ
+    s->cluster_max = s->C->session_cluster_max;                    // ... or PBRCM_SESSION_CLUSTER_MAX
     if (const char* e = std::getenv("PBRCM_SESSION_TEAM_MIN"))
         s->team_min = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("PBRCM_SESSION_TEAM_MAX"))
@@ -748,8 +748,6 @@ int32_t pbrcm_session_create(pbrcm_context* ctx, const pbrcm_session_config* cfg
     }
     if (const char* e = std::getenv("PBRCM_SESSION_TRACE"))
         s->trace_path = e;
-    if (const char* e = std::getenv("PBRCM_SESSION_CLUSTER_MAX"))
-        s->cluster_max = std::max(0, std::min(16, std::atoi(e)));
     if (cudaDeviceGetDefaultMemPool(&s->pool, s->C->device) != cudaSuccess) {
         delete s;
         return PBRCM_ERR_CUDA;

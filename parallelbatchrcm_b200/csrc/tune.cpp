@@ -59,6 +59,8 @@ pbrcm_tuning from_context(const Context& C)
     t.cluster_nnz = (uint32_t)std::min<uint64_t>(C.cluster_nnz, 0xFFFFFFFFu);
     t.session_cutoff_n = C.session_cutoff_n;
     t.session_pool = (uint32_t)C.session_pool;
+    t.session_team_nnz = C.session_team_nnz;
+    t.session_cluster_max = (uint32_t)C.session_cluster_max;
     t.sms = (uint32_t)C.sms;
     t.source = C.tuned;
     return t;
@@ -67,7 +69,8 @@ pbrcm_tuning from_context(const Context& C)
 bool valid(const pbrcm_tuning& t)
 {
     return batch_pool_ok((int)t.batch_pool) && t.batch_kernel <= 1 && t.cluster_size >= 1 && t.cluster_size <= 16 && t.cluster_nnz >= 1 &&
-           t.session_cutoff_n >= 1 && session_pool_ok((int)t.session_pool);
+           t.session_cutoff_n >= 1 && session_pool_ok((int)t.session_pool) && t.session_team_nnz >= 1 &&
+           t.session_cluster_max <= 16 && t.session_cluster_max != 1;
 }
 
 void to_context(Context& C, const pbrcm_tuning& t)
@@ -79,6 +82,8 @@ void to_context(Context& C, const pbrcm_tuning& t)
     C.cluster_nnz = t.cluster_nnz;
     C.session_cutoff_n = t.session_cutoff_n;
     C.session_pool = (int)t.session_pool;
+    C.session_team_nnz = t.session_team_nnz;
+    C.session_cluster_max = (int)t.session_cluster_max;
     // solo bounds of a cluster team follow the pool's CTA shape
     C.cluster_solo_parents = (uint32_t)kPools[C.batch_pool].block;
     C.cluster_solo_edges = (uint32_t)kPools[C.batch_pool].emax;
@@ -91,10 +96,11 @@ bool write_file(const char* path, const pbrcm_tuning& t)
         return false;
     std::fprintf(f,
                  "%s\nversion=%s\nsms=%u\nbatch_pool=%u\nbatch_kernel=%u\ncluster_size=%u\ncluster_max=%u\ncluster_nnz=%u\n"
-                 "session_cutoff_n=%u\nsession_pool=%u\ntrials=%u\ndefault_ms=%.4f\nbest_ms=%.4f\n"
+                 "session_cutoff_n=%u\nsession_pool=%u\nsession_team_nnz=%u\nsession_cluster_max=%u\n"
+                 "trials=%u\ndefault_ms=%.4f\nbest_ms=%.4f\n"
                  "session_default_ms=%.4f\nsession_best_ms=%.4f\n",
                  kTuningMagic, kVersion, t.sms, t.batch_pool, t.batch_kernel, t.cluster_size, t.cluster_max, t.cluster_nnz,
-                 t.session_cutoff_n, t.session_pool, t.trials, t.default_ms, t.best_ms, t.session_default_ms,
+                 t.session_cutoff_n, t.session_pool, t.session_team_nnz, t.session_cluster_max, t.trials, t.default_ms, t.best_ms, t.session_default_ms,
                  t.session_best_ms);
     return std::fclose(f) == 0;
 }
@@ -126,6 +132,8 @@ bool pbrcm::load_tuning_file(const char* path, int sms, pbrcm_tuning* out)
     bool magic = false, version = false;
     pbrcm_tuning t;
     std::memset(&t, 0, sizeof(t));
+    t.session_team_nnz = 1u << 20;  // keys a file may lack
+    t.session_cluster_max = 16;
     while (std::fgets(line, sizeof(line), f)) {
         std::string s(line);
         while (!s.empty() && (s.back() == '\n' || s.back() == '\r'))
@@ -157,6 +165,10 @@ bool pbrcm::load_tuning_file(const char* path, int sms, pbrcm_tuning* out)
             t.session_cutoff_n = (uint32_t)u;
         else if (k == "session_pool")
             t.session_pool = (uint32_t)u;
+        else if (k == "session_team_nnz")
+            t.session_team_nnz = (uint32_t)u;
+        else if (k == "session_cluster_max")
+            t.session_cluster_max = (uint32_t)u;
         else if (k == "trials")
             t.trials = (uint32_t)u;
         else if (k == "default_ms")
@@ -340,15 +352,17 @@ int32_t pbrcm_autotune(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t co
     cudaFree(D);
     lk.unlock();
 
-    // 4. serving cutoff: the batch replayed through a session (host buffers,
+    // 4. serving cutoff and CTA shape: the batch replayed through a session (host buffers,
     // all requests at once), makespan; results must equal the batch's
     float sdef = 0.f, sbest = 0.f;
     if (rc == PBRCM_OK) {
-        auto replay = [&](uint32_t cutoff, uint32_t pool, float& ms) -> int32_t {
+        auto replay = [&](uint32_t cutoff, uint32_t pool, uint32_t team_nnz, uint32_t cmax, float& ms) -> int32_t {
             {
                 std::lock_guard<std::mutex> g(C.mu);
                 C.session_cutoff_n = cutoff;
                 C.session_pool = (int)pool;
+                C.session_team_nnz = team_nnz;
+                C.session_cluster_max = (int)cmax;
             }
             pbrcm_session* s = nullptr;
             int32_t e = pbrcm_session_create(ctx, nullptr, &s);
@@ -377,7 +391,8 @@ int32_t pbrcm_autotune(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t co
         };
         const uint32_t start_cut = best.session_cutoff_n;
         const uint32_t start_pool = best.session_pool;
-        rc = replay(start_cut, start_pool, sdef);
+        const uint32_t tnnz = best.session_team_nnz, cmax = best.session_cluster_max;
+        rc = replay(start_cut, start_pool, tnnz, cmax, sdef);
         sbest = sdef;
         for (uint32_t pool : {0u, 4u, 5u, 6u})
             for (uint32_t sh : {16u, 17u, 18u, 19u, 20u}) {
@@ -385,16 +400,33 @@ int32_t pbrcm_autotune(pbrcm_context* ctx, const pbrcm_matrix* mats, uint32_t co
                 if (rc != PBRCM_OK || (cut == start_cut && pool == start_pool))
                     continue;
                 float ms = 0.f;
-                rc = replay(cut, pool, ms);
+                rc = replay(cut, pool, tnnz, cmax, ms);
                 if (rc == PBRCM_OK && ms < sbest * 0.97f) {
                     sbest = ms;
                     best.session_cutoff_n = cut;
                     best.session_pool = pool;
                 }
             }
+        // 5. the teams of big requests: CTAs per entry and the largest
+        // thread-block-cluster team
+        for (uint32_t cm : {0u, 8u, 16u})
+            for (uint32_t sh : {19u, 20u, 21u}) {
+                const uint32_t tn = 1u << sh;
+                if (rc != PBRCM_OK || (tn == tnnz && cm == cmax))
+                    continue;
+                float ms = 0.f;
+                rc = replay(best.session_cutoff_n, best.session_pool, tn, cm, ms);
+                if (rc == PBRCM_OK && ms < sbest * 0.97f) {
+                    sbest = ms;
+                    best.session_team_nnz = tn;
+                    best.session_cluster_max = cm;
+                }
+            }
         std::lock_guard<std::mutex> g(C.mu);
         C.session_cutoff_n = best.session_cutoff_n;
         C.session_pool = (int)best.session_pool;
+        C.session_team_nnz = best.session_team_nnz;
+        C.session_cluster_max = (int)best.session_cluster_max;
     }
     if (rc != PBRCM_OK)
         return rc;

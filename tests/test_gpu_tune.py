@@ -42,7 +42,7 @@ def test_autotune_keeps_permutations(pbrcm, tmp_path):
             pbrcm.tuning_load(ctx2, path)
             t2 = pbrcm.tuning_get(ctx2)
             for k in ("batch_pool", "batch_kernel", "cluster_size", "cluster_max", "cluster_nnz", "session_cutoff_n",
-                      "session_pool"):
+                      "session_pool", "session_team_nnz", "session_cluster_max"):
                 assert t2[k] == t[k], k
             assert t2["source"] == 1
             text = open(path).read().replace(f"sms={t['sms']}", f"sms={t['sms'] + 1}")
