@@ -356,16 +356,24 @@ struct Team {
     // ran out).
     __device__ bool sync(uint32_t where)
     {
-        int& s_ok = sh[1];
         if (gs == nullptr)
             return block_ok();
         target += 1;
+        // this barrier's verdict, in one of two slots by parity (the next
+        // barrier resets the other one, so no thread reading this one meets
+        // the reset and no barrier is needed after the read)
+        int& s_ok = sh[(target & 1u) ? 1 : 10];
         if (tid == 0)
             s_ok = 1;
         gbar();
         if (mode == 0) {
             if (tid == 0) {
                 red_release_add(&gs->count, 1u);
+                // the status read goes out with the polls, not after them:
+                // an error posted before this CTA arrived is seen here, one
+                // posted later at the next barrier or bounded wait (each
+                // checks the status)
+                const uint32_t st0 = read_status(res);
                 const uint32_t goal = target * expected;
                 unsigned long long t0 = 0;
                 uint32_t spins = 0;
@@ -377,7 +385,11 @@ struct Team {
                     if (spins > 2048)
                         __nanosleep(128);
                 }
+                if (st0 != 0)
+                    s_ok = 0;
             }
+            gbar();
+            return s_ok != 0;
         } else {
             if (tid == 0)
                 st_release(flags + rank, target);
