@@ -93,7 +93,8 @@ typedef struct pbrcm_result {
     float device_ms;             /* device time of the reorder launch(es) */
     float total_ms;              /* host wall time of the call */
     uint32_t engine;             /* 0: team engine (one cooperative launch); 1: level-synchronous
-                                    engine for wide, shallow graphs (same result) */
+                                    engine for wide, shallow graphs; 2: shared-memory engine for
+                                    matrices that fit one CTA's shared memory (same result) */
     uint32_t reserved;
 } pbrcm_result;
 

@@ -147,14 +147,23 @@ int32_t Context::init(int dev)
     barrier = (uint32_t)env_int("PBRCM_BARRIER", 0) ? 1u : 0u;
     spec_from = (uint32_t)std::max(0, env_int("PBRCM_SPEC_FROM", 3));
     // wide, shallow graphs: PBRCM_WIDE_DIV (0: never), PBRCM_WIDE_MIN,
-    // PBRCM_ENGINE=wide to run the level-synchronous engine first
+    // PBRCM_ENGINE=wide to run the level-synchronous engine first, =team for
+    // the team engine alone
     wide_div = (uint32_t)std::max(0, env_int("PBRCM_WIDE_DIV", 16));
     wide_min = (uint32_t)std::max(1, env_int("PBRCM_WIDE_MIN", 1 << 18));
-    if (const char* e = std::getenv("PBRCM_ENGINE"))
+    if (const char* e = std::getenv("PBRCM_ENGINE")) {
         wide_force = std::string(e) == "wide";
+        team_force = std::string(e) == "team";
+    }
     wide_fused = env_int("PBRCM_WIDE_FUSED", 1) != 0;
     wide_batch_pass = env_int("PBRCM_WIDE_BATCH_PASS", 1) != 0;
     wide_ctas = wide_ctas_per_sm() * sms;
+    // small matrices: the shared-memory engine (PBRCM_RESIDENT_GROUP: 32,
+    // 64, 128 or 256 threads a group; 0 off)
+    resident_group = env_int("PBRCM_RESIDENT_GROUP", 128);
+    if (!resident_group_ok(resident_group))
+        resident_group = 0;
+    resident_max_smem = (int)prop.sharedMemPerBlockOptin - 2048;  // room for its static shared memory
     // batch / serving shape: built-in defaults (measured on the 4,096-matrix
     // mixed batch on a B200: the solo batch kernel with three 256-thread
     // CTAs per SM, 82 ms; 2 x 256 threads per CTA, 86 ms with the solo
@@ -334,8 +343,33 @@ bool Context::run_wide(const MatrixView& M, const Options& opt, cudaStream_t st)
 int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint64_t nnz, uint32_t* perm,
                             const Options& opt, cudaStream_t st, DevResult* out, float* dev_ms)
 {
+    // a matrix whose CSR and workspace fit one CTA's shared memory: the
+    // shared-memory engine, which checks the CSR itself; a row longer than
+    // its chunks sends the matrix on to the engines below
+    // (not when an engine is forced, nor under the phantom-CTA test hook,
+    // which tests the team's barrier)
+    if (resident_group > 0 && !wide_force && !team_force && opt.phantom == 0 && n >= 1 &&
+        resident_smem(resident_group, n, (uint32_t)nnz, false) <= (size_t)resident_max_smem) {
+        if (cudaMemsetAsync(d_res, 0, sizeof(DevResult), st) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+        cudaEventRecord(ev0, st);
+        if (launch_resident(resident_group, rp, ci, n, (uint32_t)nnz, perm, d_res, opt, resident_max_smem, st) !=
+            cudaSuccess)
+            return PBRCM_ERR_CUDA;
+        cudaEventRecord(ev1, st);
+        if (cudaMemcpyAsync(h_res, d_res, sizeof(DevResult), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+        if (h_res->status != kNeedTeam) {
+            if (dev_ms)
+                cudaEventElapsedTime(dev_ms, ev0, ev1);
+            *out = *h_res;
+            out->engine = 2;
+            return PBRCM_OK;
+        }
+    }
     bool with_hub = false;
-    bool try_wide = wide_ctas > 0 && wide_div != 0 && n > 1;
+    bool try_wide = wide_ctas > 0 && wide_div != 0 && n > 1 && !team_force;
     bool wide_first = try_wide && wide_force;
     for (int attempt = 0; attempt < 4; ++attempt) {
         MatrixView M{};

@@ -37,9 +37,14 @@ struct Context {
     // the matrix over; wide_force runs it first (rows permitting)
     uint32_t wide_div = 16, wide_min = 1u << 18;
     bool wide_force = false;
+    bool team_force = false;  // PBRCM_ENGINE=team: no shared-memory engine, no hand-over
     bool wide_fused = true;        // the place kernel's last CTA advances the level state
     bool wide_batch_pass = true;   // batches sized by the last pass's levels (else 8, 16, 32, ...)
     int wide_ctas = 0;  // CTAs per level step (0: engine unavailable)
+    // the shared-memory engine (resident.cu) for matrices whose CSR and
+    // workspace fit one CTA's shared memory: group size (64, 128, 256; 0 off)
+    int resident_group = 128;
+    int resident_max_smem = 0;  // dynamic shared memory a CTA may take
     // batches: the biggest matrices go to thread-block-cluster teams
     int cluster_size = 1;             // CTAs per cluster (0 or 1: off)
     uint64_t cluster_nnz = 1u << 18;  // matrices with at least this many entries

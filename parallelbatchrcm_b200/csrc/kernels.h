@@ -57,6 +57,17 @@ int solo_max_ctas(int p, int sms);
 cudaError_t launch_solo(int p, const BatchJob* jobs, const BatchSlot* slots, uint32_t nslots, uint32_t* counter,
                         const Options& opt, int ctas, cudaStream_t st);
 
+// The shared-memory engine (resident.cu): one CTA of two groups of g
+// threads (32, 64, 128 or 256) holds the matrix in shared memory and runs the
+// whole reorder.  resident_smem: dynamic shared memory for one (spec false)
+// or two workspaces; the launch takes two when they fit max_smem.  Rows of
+// more than kResidentMaxRow entries are refused on the device (kNeedTeam).
+constexpr uint32_t kResidentMaxRow = 512;
+bool resident_group_ok(int g);
+size_t resident_smem(int g, uint32_t n, uint32_t nnz, bool spec);
+cudaError_t launch_resident(int g, const uint32_t* rp, const uint32_t* ci, uint32_t n, uint32_t nnz, uint32_t* perm,
+                            DevResult* res, const Options& opt, int max_smem, cudaStream_t st);
+
 cudaError_t launch_validate(const uint32_t* rp, const uint32_t* ci, uint32_t n, uint32_t nnz, DevResult* res,
                             int sms, cudaStream_t st);
 cudaError_t launch_team(int v, const MatrixView& M, const Options& opt, GridSync* gs, unsigned long long* agg,

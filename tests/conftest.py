@@ -47,3 +47,24 @@ def gpu_ctx(pbrcm):
     ctx = pbrcm.Context(0)
     yield ctx
     ctx.close()
+
+
+@pytest.fixture(scope="session")
+def gpu_ctx_team(pbrcm):
+    """A context that runs every single matrix on the team engine
+    (PBRCM_ENGINE=team: neither the shared-memory engine nor the hand-over
+    to the level-synchronous one)."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    old = os.environ.get("PBRCM_ENGINE")
+    os.environ["PBRCM_ENGINE"] = "team"
+    try:
+        ctx = pbrcm.Context(0)
+    finally:
+        if old is None:
+            del os.environ["PBRCM_ENGINE"]
+        else:
+            os.environ["PBRCM_ENGINE"] = old
+    yield ctx
+    ctx.close()

@@ -8,10 +8,17 @@ from conftest import golden_names, load_golden
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=["default", "team"])
+def any_ctx(request, gpu_ctx, gpu_ctx_team):
+    """The default context (small matrices on the shared-memory engine) and
+    one that keeps every matrix on the team engine."""
+    return gpu_ctx if request.param == "default" else gpu_ctx_team
+
+
 @pytest.mark.parametrize("name", golden_names())
-def test_golden_auto_start(pbrcm, gpu_ctx, name):
+def test_golden_auto_start(pbrcm, any_ctx, name):
     g = load_golden(name)
-    perm, res = pbrcm.reorder(g["row_ptr"], g["col_idx"], reverse=False, ctx=gpu_ctx)
+    perm, res = pbrcm.reorder(g["row_ptr"], g["col_idx"], reverse=False, ctx=any_ctx)
     assert res["status"] == 0
     assert (res["start_node"], res["peripheral_passes"], res["eccentricity"]) == (
         int(g["start"]), int(g["passes"]), int(g["ecc"]))
@@ -21,9 +28,9 @@ def test_golden_auto_start(pbrcm, gpu_ctx, name):
 
 
 @pytest.mark.parametrize("name", golden_names())
-def test_golden_reverse_and_profile(pbrcm, gpu_ctx, oracle_mod, name):
+def test_golden_reverse_and_profile(pbrcm, any_ctx, oracle_mod, name):
     g = load_golden(name)
-    perm, res = pbrcm.reorder(g["row_ptr"], g["col_idx"], reverse=True, ctx=gpu_ctx)
+    perm, res = pbrcm.reorder(g["row_ptr"], g["col_idx"], reverse=True, ctx=any_ctx)
     assert np.array_equal(perm, g["perm"][::-1])
     assert res["bandwidth"] == int(g["bandwidth"])
     assert res["profile"] == oracle_mod.profile(g["row_ptr"], g["col_idx"], perm)
@@ -31,12 +38,12 @@ def test_golden_reverse_and_profile(pbrcm, gpu_ctx, oracle_mod, name):
 
 @pytest.mark.parametrize("name", ["grid2d_64x64_s1", "rgg_3000_s11", "star_1500_ring7", "caterpillar_40x60",
                                   "mtx_general_dups", "path_300"])
-def test_explicit_starts_match_oracle(pbrcm, gpu_ctx, oracle_mod, name):
+def test_explicit_starts_match_oracle(pbrcm, any_ctx, oracle_mod, name):
     g = load_golden(name)
     n = g["row_ptr"].shape[0] - 1
     rng = np.random.default_rng(7)
     for s in sorted(set([0, n - 1] + list(rng.integers(0, n, 4)))):
-        perm, res = pbrcm.reorder(g["row_ptr"], g["col_idx"], reverse=False, start=int(s), ctx=gpu_ctx)
+        perm, res = pbrcm.reorder(g["row_ptr"], g["col_idx"], reverse=False, start=int(s), ctx=any_ctx)
         assert res["start_node"] == s and res["peripheral_passes"] == 0
         assert np.array_equal(perm, oracle_mod.cm_order(g["row_ptr"], g["col_idx"], int(s)))
 
