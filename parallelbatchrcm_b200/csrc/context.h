@@ -42,8 +42,9 @@ struct Context {
     bool wide_batch_pass = true;   // batches sized by the last pass's levels (else 8, 16, 32, ...)
     int wide_ctas = 0;  // CTAs per level step (0: engine unavailable)
     // the shared-memory engine (resident.cu) for matrices whose CSR and
-    // workspace fit one CTA's shared memory: group size (64, 128, 256; 0 off)
-    int resident_group = 128;
+    // workspace fit one CTA's shared memory: group size (32, 64, 128, 256;
+    // 0 off; -1 chosen per matrix)
+    int resident_group = -1;
     int resident_max_smem = 0;  // dynamic shared memory a CTA may take
     // batches: the biggest matrices go to thread-block-cluster teams
     int cluster_size = 1;             // CTAs per cluster (0 or 1: off)

@@ -12,8 +12,9 @@
 // touches shared memory only.
 //
 // Layout (dynamic shared memory): two groups' chunk scratch, row_ptr (n + 1
-// words), col_idx (nnz), and per group a claim word and a queue slot per node
-// (2 x 4n bytes; the second group's only when the speculative pass is on).
+// words), col_idx (nnz), per group a claim word and a queue slot per node
+// (2 x 4n bytes; the second group's only when the speculative pass is on),
+// and a valence byte per node.
 //
 // One BFS pass (res_pass) walks the FIFO queue in chunks of at most G parents
 // and EW = G x R edges (never across a level boundary).  Per chunk: each
@@ -63,13 +64,14 @@ struct ResGroup {
     uint32_t* q;         // shared memory, n: the queue
     uint32_t n, nnz;
     DevResult* res;
+    const uint8_t* dg;   // shared memory, n: valence per node (rows of at most 255 entries)
 };
 
 // One BFS pass from `start` by one group; the queue ends up in g.q[0 ..
 // placed).  nlevels: levels of the pass; last_start: first position of its
 // last level.
 template <int G, int R>
-__device__ __forceinline__ void res_pass(ResGroup<G, R>& g, uint32_t start, bool sorted, uint32_t& placed, uint32_t& nlevels,
+__device__ void res_pass(ResGroup<G, R>& g, uint32_t start, bool sorted, uint32_t& placed, uint32_t& nlevels,
                          uint32_t& last_start)
 {
     constexpr uint32_t EW = (uint32_t)(G * R), W = (uint32_t)(G / 32);
@@ -238,12 +240,13 @@ __device__ __forceinline__ void res_pass(ResGroup<G, R>& g, uint32_t start, bool
     last_start = lstart;
 }
 
-// Matrices whose rows all have at most ROW entries (8 or 16): the same pass
+// Matrices whose rows all have at most ROW entries (6, 8 or 16): the same pass
 // with one parent per thread and the row in registers.  Thread j loads its
 // parent's whole row at once (the loop over slots is unrolled, so every load
 // of the row is in flight together) and slot k bids kResClaim | j << 5 | k
 // (the (parent, slot) order of the chunk), so no edge needs its parent looked
-// up; the children's valences are loaded beside the bids.  After the barrier
+// up; the children's valences (a byte table built with the CSR check) are
+// loaded beside the bids.  After the barrier
 // the thread tests its own bids into a bit mask, one scan gives each parent
 // its first queue position, and the thread writes its children in slot order
 // or ranked by (valence, slot) among themselves -- register arithmetic.
@@ -258,6 +261,12 @@ __device__ __forceinline__ uint32_t lds(uint32_t a)
     asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
     return v;
 }
+__device__ __forceinline__ uint32_t ldsb(uint32_t a)
+{
+    uint32_t v;
+    asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+    return v;
+}
 __device__ __forceinline__ void sts(uint32_t a, uint32_t v)
 {
     asm volatile("st.shared.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
@@ -268,7 +277,7 @@ __device__ __forceinline__ void reds_min(uint32_t a, uint32_t v)
 }
 
 template <int G, int R, int ROW>
-__device__ __forceinline__ void res_pass_short(ResGroup<G, R>& g, uint32_t start, bool sorted, uint32_t& placed, uint32_t& nlevels,
+__device__ __noinline__ void res_pass_short(ResGroup<G, R>& g, uint32_t start, bool sorted, uint32_t& placed, uint32_t& nlevels,
                                uint32_t& last_start)
 {
     static_assert(ROW <= 32 && G <= 1024, "slot bits and parent bits of a bid");
@@ -285,7 +294,7 @@ __device__ __forceinline__ void res_pass_short(ResGroup<G, R>& g, uint32_t start
     gsync<G>();
     uint32_t head = 0, tail = 1, lvl_end = 1, L = 0, lstart = 0;
     const uint32_t key0 = kResClaim | (t << 5);
-    const uint32_t qa = saddr(g.q), wa = saddr(g.w), rpa = saddr(g.rp), cia = saddr(g.ci);
+    const uint32_t qa = saddr(g.q), wa = saddr(g.w), rpa = saddr(g.rp), cia = saddr(g.ci), dga = saddr(g.dg);
     while (head < tail) {
         if (head == lvl_end) {
             L += 1;
@@ -315,7 +324,9 @@ __device__ __forceinline__ void res_pass_short(ResGroup<G, R>& g, uint32_t start
                 if (c[k] != kUnvisited && PB_CHECK(g.res, c[k] < n, 627)) {
                     reds_min(wa + 4 * c[k], key0 | (uint32_t)k);
                     if (sorted)
-                        d[k] = lds(rpa + 4 * (c[k] + 1)) - lds(rpa + 4 * c[k]);
+                        d[k] = ldsb(dga + c[k]);
+                } else {
+                    c[k] = kUnvisited;
                 }
             }
         }
@@ -325,7 +336,7 @@ __device__ __forceinline__ void res_pass_short(ResGroup<G, R>& g, uint32_t start
         if (wbusy) {
 #pragma unroll
             for (int k = 0; k < ROW; ++k)
-                if (c[k] != kUnvisited && c[k] < n && lds(wa + 4 * c[k]) == (key0 | (uint32_t)k))
+                if (c[k] != kUnvisited && lds(wa + 4 * c[k]) == (key0 | (uint32_t)k))
                     win |= 1u << k;
         }
         uint32_t Q;
@@ -422,7 +433,8 @@ __device__ __forceinline__ void cp_async4(uint32_t* dst, const uint32_t* src)
 template <int G, int R>
 PBRCM_HD inline size_t res_smem(uint32_t n, uint32_t nnz, bool spec)
 {
-    return 2 * sizeof(ResScratch<G, R>) + 4 * ((size_t)n + 1 + (size_t)nnz) + (spec ? 16 : 8) * (size_t)n;
+    return 2 * sizeof(ResScratch<G, R>) + 4 * ((size_t)n + 1 + (size_t)nnz) + (spec ? 16 : 8) * (size_t)n +
+           (((size_t)n + 3) & ~(size_t)3);
 }
 
 // One matrix, one CTA of two groups.  spec: room for the second workspace.
@@ -444,6 +456,7 @@ __global__ void __launch_bounds__(2 * G, 1)
     uint32_t* q0 = w0 + n;
     uint32_t* w1 = spec ? q0 + n : w0;
     uint32_t* q1 = spec ? w1 + n : q0;
+    uint8_t* dg8 = reinterpret_cast<uint8_t*>((spec ? q1 : q0) + n);
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
     const uint32_t grp = tid / G;
     if (tid == 0)
@@ -460,10 +473,12 @@ __global__ void __launch_bounds__(2 * G, 1)
     uint32_t mx = 0;
     for (uint32_t i = tid; i < n; i += nthr) {
         const uint32_t a = rp[i], b = rp[i + 1];
-        if (b < a || b > nnz)
+        if (b < a || b > nnz) {
             bad = true;
-        else
+        } else {
             mx = max(mx, b - a);
+            dg8[i] = (uint8_t)min(b - a, 255u);
+        }
     }
     if (tid == 0 && (rp[0] != 0 || rp[n] != nnz))
         bad = true;
@@ -499,10 +514,10 @@ __global__ void __launch_bounds__(2 * G, 1)
     } else if (searching) {
         start = n / 2;
     }
-    ResGroup<G, R> gr{scr[grp], rp, ci, grp ? w1 : w0, grp ? q1 : q0, n, nnz, res};
+    ResGroup<G, R> gr{scr[grp], rp, ci, grp ? w1 : w0, grp ? q1 : q0, n, nnz, res, dg8};
     const uint32_t sorter = spec ? 1u : 0u;  // the group that runs sorted passes
-    // rows of at most 8 or 16 entries: the one-parent-a-thread pass
-    const uint32_t row_class = maxdeg <= 8 ? 8u : maxdeg <= 16 ? 16u : 0u;
+    // rows of at most 6, 8 or 16 entries: the one-parent-a-thread pass
+    const uint32_t row_class = maxdeg <= 6 ? 6u : maxdeg <= 8 ? 8u : maxdeg <= 16 ? 16u : 0u;
     uint32_t lastdist = 0, sorted_from = kUnvisited, s_placed = 0, s_levels = 0;
     // rounds: group 0 runs a start-search pass while (with spec) group 1
     // runs the sorted pass from the same start, from the second search on
@@ -514,7 +529,9 @@ __global__ void __launch_bounds__(2 * G, 1)
         const bool run_sort = opt.mode != kModeStartOnly && (!searching || (spec && passes >= 1));
         if (run_search && grp == 0) {
             uint32_t pl, nl, ls;
-            if (row_class == 8)
+            if (row_class == 6)
+                res_pass_short<G, R, 6>(gr, start, false, pl, nl, ls);
+            else if (row_class == 8)
                 res_pass_short<G, R, 8>(gr, start, false, pl, nl, ls);
             else if (row_class == 16)
                 res_pass_short<G, R, 16>(gr, start, false, pl, nl, ls);
@@ -528,7 +545,9 @@ __global__ void __launch_bounds__(2 * G, 1)
         }
         if (run_sort && grp == sorter) {
             uint32_t pl, nl, ls;
-            if (row_class == 8)
+            if (row_class == 6)
+                res_pass_short<G, R, 6>(gr, start, true, pl, nl, ls);
+            else if (row_class == 8)
                 res_pass_short<G, R, 8>(gr, start, true, pl, nl, ls);
             else if (row_class == 16)
                 res_pass_short<G, R, 16>(gr, start, true, pl, nl, ls);
