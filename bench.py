@@ -25,8 +25,9 @@ sum over ranks of reorders / the max over ranks of the timed time.
 
 --workload single|batch|serve|permute|connect|wide run one part alone;
 refgpu times the reference's own GPU_SIMPLE beside this engine, cpu the
-reference's serial and CPU_BATCH paths on the single-matrix configurations
-(bench_workloads.py).
+reference's serial and CPU_BATCH paths on the single-matrix configurations,
+small the shared-memory engine on small matrices (the 64^2 grid first) beside
+the team engine and the reference's serial code (bench_workloads.py).
 """
 from __future__ import annotations
 
@@ -47,7 +48,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed",
-                    choices=["mixed", "single", "batch", "serve", "permute", "connect", "wide", "refgpu", "cpu"])
+                    choices=["mixed", "single", "batch", "serve", "permute", "connect", "wide", "refgpu", "cpu",
+                             "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lean", action="store_true",
                     help="batched launches only (no plain pass, e2e, serving, 128^3 grid or CPU legs): for profiling")

@@ -19,6 +19,8 @@ batch  the many-matrix batch alone (any count: PBRCM_BENCH_COUNT).
 serve  the serving sweep alone (PBRCM_SERVE_COUNT requests, PBRCM_SERVE_RATES).
 permute / connect / wide   P A P^T, the loader's connectivity repair, and a
        wide random graph (level-synchronous engine).
+small  small matrices (the 64^2 grid first) on the shared-memory engine
+       beside the team engine and the reference's serial CPU code.
 
 Under torchrun each rank takes its own share: the batch stream has
 4,096 matrices per GPU (weak scaling, no exchange between GPUs); one matrix
@@ -1069,6 +1071,88 @@ def run_refgpu(args, ws, rank, local):
     return 0
 
 
+def _small_configs():
+    """Matrices the shared-memory engine takes, the 64^2 grid first."""
+    return [("grid2d_64x64", lambda: gen.grid2d(64, 64, seed=1)),
+            ("grid2d_32x32", lambda: gen.grid2d(32, 32, seed=2)),
+            ("grid3d_16^3", lambda: gen.grid3d(16, 16, 16, seed=4)),
+            ("grid2d_90x60", lambda: gen.grid2d(90, 60, seed=6)),
+            ("rgg_3000_k4-12", lambda: gen.rgg(3000, kmin=4, kmax=12, seed=5))]
+
+
+def run_small(args, ws, rank, local):
+    """Small matrices, one at a time (rank 0): full reorders (start search +
+    RCM + bandwidth) on the default context -- the shared-memory engine --
+    device-resident (CUDA events on the launching stream, median of --steps
+    after --warmup) and end to end from host buffers through pbrcm_reorder
+    (its own wall time), beside the team engine alone (PBRCM_ENGINE=team) and
+    the reference's own findPeripheral + rcm_seq on one host thread.  Every
+    permutation is checked against the oracle."""
+    import torch
+
+    import parallelbatchrcm_b200 as P
+    if rank != 0:
+        return 0
+    O = _oracle()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = P.Context(local)
+    old = os.environ.get("PBRCM_ENGINE")
+    os.environ["PBRCM_ENGINE"] = "team"
+    try:
+        team = P.Context(local)
+    finally:
+        if old is None:
+            os.environ.pop("PBRCM_ENGINE")
+        else:
+            os.environ["PBRCM_ENGINE"] = old
+    st = torch.cuda.Stream(device=dev)
+    rows = []
+    for name, make in _small_configs():
+        m = make()
+        ref = O.full_reorder(m.row_ptr, m.col_idx, reverse=True)
+        rp = torch.from_numpy(m.row_ptr.view(np.int32)).to(dev)
+        ci = torch.from_numpy(m.col_idx.view(np.int32)).to(dev)
+        po = torch.empty(m.n, dtype=torch.int32, device=dev)
+
+        def timed(c):
+            ts = []
+            for i in range(args.warmup + args.steps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                _, r = P.reorder_device(rp, ci, po, ctx=c, stream=st)
+                e1.record(st)
+                e1.synchronize()
+                if i >= args.warmup:
+                    ts.append(e0.elapsed_time(e1))
+            ok = np.array_equal(po.cpu().numpy().view(np.uint32), ref["perm"])
+            return statistics.median(ts), r["engine"], ok
+
+        ms, engine, ok = timed(ctx)
+        tms, tengine, tok = timed(team)
+        hp = np.empty(m.n, dtype=np.uint32)
+        e2e = []
+        for i in range(args.warmup + args.steps):
+            _, r = P.reorder(m.row_ptr, m.col_idx, ctx=ctx, perm_out=hp)
+            if i >= args.warmup:
+                e2e.append(r["total_ms"])
+        row = {"workload": name, "n": m.n, "nnz": m.nnz, "engine": engine, "ms": ms,
+               "e2e_ms": statistics.median(e2e), "team_ms": tms,
+               "equals_oracle": bool(ok and tok and np.array_equal(hp, ref["perm"])), "team_engine": tengine}
+        if O.ref_available():
+            rr = O.ref_time(m.row_ptr, m.col_idx, 1, 1)[0]
+            row.update({"reference_peripheral_ms": rr["peripheral_ms"], "reference_rcm_ms": rr["rcm_ms"],
+                        "reference_ms": rr["peripheral_ms"] + rr["rcm_ms"]})
+        rows.append(row)
+        log(json.dumps(row))
+    ctx.close()
+    team.close()
+    print(json.dumps({"metric": "ms per full reorder of a small matrix: shared-memory engine (device, end to end) "
+                                "vs team engine vs the reference's serial CPU code (1 thread)",
+                      "rows": rows}), flush=True)
+    return 0
+
+
 def run_cpu(args, ws, rank, local):
     """The reference's CPU paths on the single-matrix configurations, on this
     host: findPeripheral + RealCPU::rcm<true> serial (rcm_seq) and CPU_BATCH
@@ -1114,7 +1198,8 @@ def main(args, ws, rank, local):
             return run_single_reference(args, ws, rank)
         return run_mixed_reference(args, ws, rank)
     fn = {"mixed": run_mixed, "single": run_single, "serve": run_serve, "permute": run_permute,
-          "connect": run_connect, "wide": run_wide, "refgpu": run_refgpu, "cpu": run_cpu}.get(args.workload)
+          "connect": run_connect, "wide": run_wide, "refgpu": run_refgpu, "cpu": run_cpu,
+          "small": run_small}.get(args.workload)
     if args.workload == "batch":
         return run_mixed(args, ws, rank, local, extras=False)
     if fn is None:
