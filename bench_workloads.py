@@ -10,7 +10,8 @@ mixed (default)  The metric's own configuration: 4,096 independent matrices,
        through pbrcm_reorder_batch from pinned host buffers, the roofline of
        the batch launch, the serving session on a Poisson stream of requests
        (n in [1e3, 2e6], seed 99) against a plain FIFO worker, and the
-       single-matrix 128^3 grid as an extra key.  cpu_baseline: the
+       single-matrix 128^3 grid and the 64^2 grid (shared-memory engine, the
+       reference's serial code timed beside it) as extra keys.  cpu_baseline: the
        reference's own findPeripheral + rcm_seq<true> (oracle/_ref) over the
        same 4,096 matrices on every host thread; its permutations are also
        compared with the batched ones.
@@ -573,6 +574,20 @@ def run_mixed(args, ws, rank, local, extras: bool = True):
         g3_out = measure_grid3d(P, ctx, g3, args, ws, stream, flush, dev,
                                 cpu=rank == 0 and ws == 1 and not args.no_cpu_baseline)
 
+    # the 64^2 grid alone (shared-memory engine), the reference's serial code
+    # beside it: reported, never required
+    g2_out = None
+    if extras and rank == 0 and ws == 1:
+        try:
+            team = _team_context(P, local)
+            try:
+                g2_out = _small_row(P, _oracle(), ctx, team, gen.grid2d(64, 64, seed=1), "grid2d_64x64",
+                                    3, 20, dev, stream)
+            finally:
+                team.close()
+        except Exception as e:
+            g2_out = {"workload": "grid2d_64x64", "error": str(e)[:200]}
+
     cpu = None
     ref_same = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -617,6 +632,7 @@ def run_mixed(args, ws, rank, local, extras: bool = True):
                      "algorithmic_bytes_per_launch": abytes, "traffic": traffic},
         "serve": serve,
         "grid3d_128": g3_out,
+        "grid2d_64": g2_out,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": 2 * args.steps,
@@ -1080,14 +1096,66 @@ def _small_configs():
             ("rgg_3000_k4-12", lambda: gen.rgg(3000, kmin=4, kmax=12, seed=5))]
 
 
+def _team_context(P, local):
+    """A context that keeps every single matrix on the team engine."""
+    old = os.environ.get("PBRCM_ENGINE")
+    os.environ["PBRCM_ENGINE"] = "team"
+    try:
+        return P.Context(local)
+    finally:
+        if old is None:
+            os.environ.pop("PBRCM_ENGINE")
+        else:
+            os.environ["PBRCM_ENGINE"] = old
+
+
+def _small_row(P, O, ctx, team, m, name, warmup, steps, dev, st):
+    """One small matrix: full reorders on `ctx` (the shared-memory engine)
+    device-resident (CUDA events on `st`, median) and end to end from host
+    buffers (pbrcm_reorder's own wall time, median), on `team` (the team
+    engine alone), and the reference's own findPeripheral + rcm_seq on one
+    host thread; every permutation checked against the oracle."""
+    import torch
+    ref = O.full_reorder(m.row_ptr, m.col_idx, reverse=True)
+    rp = torch.from_numpy(m.row_ptr.view(np.int32)).to(dev)
+    ci = torch.from_numpy(m.col_idx.view(np.int32)).to(dev)
+    po = torch.empty(m.n, dtype=torch.int32, device=dev)
+
+    def timed(c):
+        ts = []
+        for i in range(warmup + steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            _, r = P.reorder_device(rp, ci, po, ctx=c, stream=st)
+            e1.record(st)
+            e1.synchronize()
+            if i >= warmup:
+                ts.append(e0.elapsed_time(e1))
+        ok = np.array_equal(po.cpu().numpy().view(np.uint32), ref["perm"])
+        return statistics.median(ts), r["engine"], ok
+
+    ms, engine, ok = timed(ctx)
+    tms, tengine, tok = timed(team)
+    hp = np.empty(m.n, dtype=np.uint32)
+    e2e = []
+    for i in range(warmup + steps):
+        _, r = P.reorder(m.row_ptr, m.col_idx, ctx=ctx, perm_out=hp)
+        if i >= warmup:
+            e2e.append(r["total_ms"])
+    row = {"workload": name, "n": m.n, "nnz": m.nnz, "engine": engine, "ms": ms,
+           "e2e_ms": statistics.median(e2e), "team_ms": tms,
+           "equals_oracle": bool(ok and tok and np.array_equal(hp, ref["perm"])), "team_engine": tengine}
+    if O.ref_available():
+        rr = O.ref_time(m.row_ptr, m.col_idx, 1, 1)[0]
+        row.update({"reference_peripheral_ms": rr["peripheral_ms"], "reference_rcm_ms": rr["rcm_ms"],
+                    "reference_ms": rr["peripheral_ms"] + rr["rcm_ms"]})
+    return row
+
+
 def run_small(args, ws, rank, local):
-    """Small matrices, one at a time (rank 0): full reorders (start search +
-    RCM + bandwidth) on the default context -- the shared-memory engine --
-    device-resident (CUDA events on the launching stream, median of --steps
-    after --warmup) and end to end from host buffers through pbrcm_reorder
-    (its own wall time), beside the team engine alone (PBRCM_ENGINE=team) and
-    the reference's own findPeripheral + rcm_seq on one host thread.  Every
-    permutation is checked against the oracle."""
+    """Small matrices, one at a time (rank 0; _small_row each): the
+    shared-memory engine beside the team engine and the reference's serial
+    code."""
     import torch
 
     import parallelbatchrcm_b200 as P
@@ -1097,54 +1165,12 @@ def run_small(args, ws, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     ctx = P.Context(local)
-    old = os.environ.get("PBRCM_ENGINE")
-    os.environ["PBRCM_ENGINE"] = "team"
-    try:
-        team = P.Context(local)
-    finally:
-        if old is None:
-            os.environ.pop("PBRCM_ENGINE")
-        else:
-            os.environ["PBRCM_ENGINE"] = old
+    team = _team_context(P, local)
     st = torch.cuda.Stream(device=dev)
     rows = []
     for name, make in _small_configs():
-        m = make()
-        ref = O.full_reorder(m.row_ptr, m.col_idx, reverse=True)
-        rp = torch.from_numpy(m.row_ptr.view(np.int32)).to(dev)
-        ci = torch.from_numpy(m.col_idx.view(np.int32)).to(dev)
-        po = torch.empty(m.n, dtype=torch.int32, device=dev)
-
-        def timed(c):
-            ts = []
-            for i in range(args.warmup + args.steps):
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(st)
-                _, r = P.reorder_device(rp, ci, po, ctx=c, stream=st)
-                e1.record(st)
-                e1.synchronize()
-                if i >= args.warmup:
-                    ts.append(e0.elapsed_time(e1))
-            ok = np.array_equal(po.cpu().numpy().view(np.uint32), ref["perm"])
-            return statistics.median(ts), r["engine"], ok
-
-        ms, engine, ok = timed(ctx)
-        tms, tengine, tok = timed(team)
-        hp = np.empty(m.n, dtype=np.uint32)
-        e2e = []
-        for i in range(args.warmup + args.steps):
-            _, r = P.reorder(m.row_ptr, m.col_idx, ctx=ctx, perm_out=hp)
-            if i >= args.warmup:
-                e2e.append(r["total_ms"])
-        row = {"workload": name, "n": m.n, "nnz": m.nnz, "engine": engine, "ms": ms,
-               "e2e_ms": statistics.median(e2e), "team_ms": tms,
-               "equals_oracle": bool(ok and tok and np.array_equal(hp, ref["perm"])), "team_engine": tengine}
-        if O.ref_available():
-            rr = O.ref_time(m.row_ptr, m.col_idx, 1, 1)[0]
-            row.update({"reference_peripheral_ms": rr["peripheral_ms"], "reference_rcm_ms": rr["rcm_ms"],
-                        "reference_ms": rr["peripheral_ms"] + rr["rcm_ms"]})
-        rows.append(row)
-        log(json.dumps(row))
+        rows.append(_small_row(P, O, ctx, team, make(), name, args.warmup, args.steps, dev, st))
+        log(json.dumps(rows[-1]))
     ctx.close()
     team.close()
     print(json.dumps({"metric": "ms per full reorder of a small matrix: shared-memory engine (device, end to end) "
