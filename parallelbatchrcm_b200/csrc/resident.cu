@@ -276,6 +276,40 @@ __device__ __forceinline__ void reds_min(uint32_t a, uint32_t v)
     asm volatile("red.shared.min.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
 }
 
+// Exclusive scan over a group of values below 2^BITS: the warp part from
+// BITS independent ballots (bit-sliced counts) instead of five dependent
+// shuffles; same buffer rule as block_scan1 (read after its barrier, written
+// again only after another group barrier).
+template <int B, int BITS>
+__device__ __forceinline__ uint32_t block_scan_bits(uint32_t v, uint32_t& total, uint32_t* buf)
+{
+    constexpr uint32_t W = (uint32_t)(B / 32);
+    const uint32_t lane = threadIdx.x & 31u, w = gtid<B>() >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t excl = 0, wsum = 0;
+#pragma unroll
+    for (int b = 0; b < BITS; ++b) {
+        const uint32_t bal = __ballot_sync(kFull, (v >> b) & 1u);
+        excl += (uint32_t)__popc(bal & lt) << b;
+        wsum += (uint32_t)__popc(bal) << b;
+    }
+    if (lane == 0)
+        buf[w] = wsum;
+    gsync<B>();
+    uint32_t before = 0, all = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < W; ++i) {
+        const uint32_t x = buf[i];
+        before += i < w ? x : 0u;
+        all += x;
+    }
+    total = all;
+    return before + excl;
+}
+
+// bits that hold 0..x
+__host__ __device__ constexpr int res_bits(int x) { return x < 8 ? 3 : x < 16 ? 4 : x < 32 ? 5 : 6; }
+
 template <int G, int R, int ROW>
 __device__ __noinline__ void res_pass_short(ResGroup<G, R>& g, uint32_t start, bool sorted, uint32_t& placed, uint32_t& nlevels,
                                uint32_t& last_start)
@@ -340,7 +374,7 @@ __device__ __noinline__ void res_pass_short(ResGroup<G, R>& g, uint32_t start, b
                     win |= 1u << k;
         }
         uint32_t Q;
-        const uint32_t base = tail + block_scan1<G>((uint32_t)__popc(win), Q, s.scanbuf);
+        const uint32_t base = tail + block_scan_bits<G, res_bits(ROW)>((uint32_t)__popc(win), Q, s.scanbuf);
         // (every bid was tested before the scan's barrier: marking is safe)
         if (win != 0) {
             // children of one valence keep slot order: no ranking
