@@ -349,11 +349,8 @@ int32_t Context::run_single(const uint32_t* rp, const uint32_t* ci, uint32_t n, 
     // its chunks sends the matrix on to the engines below
     // (not when an engine is forced, nor under the phantom-CTA test hook,
     // which tests the team's barrier)
-    // Group size unless set: 256 threads for matrices of more than six
-    // entries a row (3-D meshes and denser: wider levels), else 128 (on a
-    // B200: the 64^2 grid 0.34 ms with 128, 0.38 with 256; a 16^3 grid 0.25
-    // against 0.22 ms, a 3,000-node random geometric graph 0.47 against 0.39)
-    const int rg = resident_group >= 0 ? resident_group : (nnz > 6 * (uint64_t)n ? 256 : 128);
+    // group size unless set: by the matrix (resident_default_group)
+    const int rg = resident_group >= 0 ? resident_group : resident_default_group(n, nnz);
     if (rg > 0 && !wide_force && !team_force && opt.phantom == 0 && n >= 1 &&
         resident_smem(rg, n, (uint32_t)nnz, false) <= (size_t)resident_max_smem) {
         if (cudaMemsetAsync(d_res, 0, sizeof(DevResult), st) != cudaSuccess)

@@ -104,6 +104,7 @@ struct DeviceSetup {
     unsigned char* base = nullptr;  // device address of g_noalloc_scratch
     int sms = 0;
     int ctas = 0;
+    int max_smem = 0;  // dynamic shared memory the shared-memory engine may take
 };
 
 std::mutex g_setup_mu;
@@ -136,6 +137,9 @@ int32_t setup_device(int dev, DeviceSetup*& out)
                 d.rc = PBRCM_ERR_CUDA;
             } else {
                 d.ctas = std::min(std::min(nb * d.sms, d.sms), kNoAllocMaxCtas);
+                int optin = 0;
+                if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess)
+                    d.max_smem = optin - 2048;  // room for its static shared memory
             }
         }
         if (d.rc != PBRCM_OK)
@@ -186,6 +190,31 @@ extern "C" int32_t pbrcm_reorder_device_noalloc(const uint32_t* d_row_ptr, const
     M.hub = nullptr;
     M.res = res;
     Options opt = make_options(opts, kModeFull);
+    // a matrix that fits one CTA's shared memory: the shared-memory engine,
+    // which needs no scratch beyond the result words (it checks the CSR
+    // itself); a row longer than its chunks goes on to the team below
+    const int rg = resident_default_group(n, nnz);
+    if (opt.phantom == 0 && d->max_smem > 0 && resident_smem(rg, n, (uint32_t)nnz, false) <= (size_t)d->max_smem) {
+        DevResult h;
+        if (cudaMemsetAsync(res, 0, sizeof(DevResult), st) != cudaSuccess ||
+            launch_resident(rg, d_row_ptr, d_col_idx, n, (uint32_t)nnz, d_perm_out, res, opt, d->max_smem, st) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(&h, res, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+        if (h.status != kNeedTeam) {
+            h.engine = 2;
+            fill_result(h, opt, result);
+            if (result) {
+                result->device_ms = h.t_end > h.t_begin ? (float)((h.t_end - h.t_begin) * 1e-6) : 0.f;
+                result->total_ms =
+                    std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            }
+            return map_status(h.status);
+        }
+        if (cudaMemsetAsync(S, 0, kOffWords + team_words_bytes(d->ctas), st) != cudaSuccess)
+            return PBRCM_ERR_CUDA;
+    }
     opt.solo_parents = 2 * kNoAllocB;
     opt.solo_edges = 2 * kNoAllocEmax;
     opt.barrier = 0;

@@ -56,6 +56,8 @@ def test_noalloc_equals_allocating_entry_point(pbrcm, gpu_ctx):
             rc, res = _noalloc(L, rp, ci, got, reverse, stream)
             assert rc == 0 and res["status"] == 0
             assert torch.equal(got, want)
+            # small matrices on the shared-memory engine (no scratch), the rest on the team
+            assert res["engine"] == (2 if n <= 4096 else 0) == ref["engine"]
             for k in ("start_node", "peripheral_passes", "eccentricity", "levels", "placed", "bandwidth",
                       "initial_bandwidth", "profile"):
                 assert res[k] == ref[k], k
